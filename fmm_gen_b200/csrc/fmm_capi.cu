@@ -1,0 +1,541 @@
+// fmm_b200 host runtime and C ABI (declared in include/fmm_b200.h).
+//
+// Reference interfaces replaced (fmm-gen):
+//   bl_dgemm                       common/dgemm/my_dgemm.c:115-210
+//   bl_dgemm_strassen_abc/ab/naive common/include/bl_dgemm.h:96-130 (generated bodies:
+//                                  meta/abc_gen_mix.py:448-472, meta/ab_gen_mix.py:430-456,
+//                                  meta/naive_gen_mix.py:412-429)
+//   fringe split + peeling         meta/common_mix.py:124-171, common/dgemm/bl_dgemm_util.c:316-353
+//   packing pool                   common/dgemm/bl_dgemm_util.c:375-394 (here: stream-ordered
+//                                  device allocations, freed after each call)
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/fmm_b200.h"
+#include "fmm_kernels.cuh"
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr int kMR = 8;  // register-tile granularity of the FMM/fringe split (bl_config.h:16-17)
+constexpr int kNR = 4;
+
+std::atomic<long long> g_launches{0};
+thread_local int t_last_error = FMM_OK;
+
+struct DevTables {
+  fmm::Prod* prods = nullptr;
+  fmm::Term* terms = nullptr;
+  int* cblk = nullptr;
+  int* ent_r = nullptr;
+  double* ent_w = nullptr;
+  bool ready = false;
+};
+
+}  // namespace
+
+struct fmm_plan {
+  int dims[3];
+  int rank;
+  std::vector<fmm::Prod> prods;
+  std::vector<fmm::Term> terms;
+  // Per C block lists of (product, coefficient), products in order: used by the scatter.
+  std::vector<int> cblk;     // 4 ints per block
+  std::vector<int> ent_r;
+  std::vector<double> ent_w;
+  int n_cblk = 0;
+  std::mutex mu;
+  DevTables dev[kMaxDevices];
+};
+
+namespace {
+
+fmm_plan* g_default_plan = nullptr;
+std::mutex g_default_mu;
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return FMM_OK;
+  if (e == cudaErrorMemoryAllocation) return FMM_E_NOMEM;
+  return FMM_E_CUDA;
+}
+
+#define FMM_CUDA_TRY(expr)                  \
+  do {                                      \
+    cudaError_t _e = (expr);                \
+    if (_e != cudaSuccess) return cuda_status(_e); \
+  } while (0)
+
+int upload_tables(fmm_plan* p, DevTables& d) {
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (d.ready) return FMM_OK;
+  FMM_CUDA_TRY(cudaMalloc(&d.prods, sizeof(fmm::Prod) * p->prods.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.terms, sizeof(fmm::Term) * p->terms.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.cblk, sizeof(int) * (p->cblk.size() ? p->cblk.size() : 1)));
+  FMM_CUDA_TRY(cudaMalloc(&d.ent_r, sizeof(int) * (p->ent_r.size() ? p->ent_r.size() : 1)));
+  FMM_CUDA_TRY(cudaMalloc(&d.ent_w, sizeof(double) * (p->ent_w.size() ? p->ent_w.size() : 1)));
+  FMM_CUDA_TRY(cudaMemcpy(d.prods, p->prods.data(), sizeof(fmm::Prod) * p->prods.size(), cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemcpy(d.terms, p->terms.data(), sizeof(fmm::Term) * p->terms.size(), cudaMemcpyHostToDevice));
+  if (!p->cblk.empty())
+    FMM_CUDA_TRY(cudaMemcpy(d.cblk, p->cblk.data(), sizeof(int) * p->cblk.size(), cudaMemcpyHostToDevice));
+  if (!p->ent_r.empty()) {
+    FMM_CUDA_TRY(cudaMemcpy(d.ent_r, p->ent_r.data(), sizeof(int) * p->ent_r.size(), cudaMemcpyHostToDevice));
+    FMM_CUDA_TRY(cudaMemcpy(d.ent_w, p->ent_w.data(), sizeof(double) * p->ent_w.size(), cudaMemcpyHostToDevice));
+  }
+  d.ready = true;
+  return FMM_OK;
+}
+
+int device_tables(const fmm_plan* cp, DevTables** out) {
+  fmm_plan* p = const_cast<fmm_plan*>(cp);
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
+  DevTables& d = p->dev[dev];
+  if (!d.ready) {
+    int rc = upload_tables(p, d);
+    if (rc != FMM_OK) return rc;
+  }
+  *out = &d;
+  return FMM_OK;
+}
+
+int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, const int* cols,
+               const double* coefs, fmm_plan** out) {
+  if (!dims || !nterms || !rows || !cols || !coefs || !out || rank <= 0) return FMM_E_INVALID;
+  if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0) return FMM_E_PLAN;
+  fmm_plan* p = new (std::nothrow) fmm_plan();
+  if (!p) return FMM_E_NOMEM;
+  std::memcpy(p->dims, dims, sizeof(p->dims));
+  p->rank = rank;
+  int pos = 0;
+  const int lim[3][2] = {{dims[0], dims[1]}, {dims[1], dims[2]}, {dims[0], dims[2]}};
+  for (int r = 0; r < rank; ++r) {
+    fmm::Prod pr{};
+    int* first[3] = {&pr.a0, &pr.b0, &pr.c0};
+    int* count[3] = {&pr.na, &pr.nb, &pr.nc};
+    for (int s = 0; s < 3; ++s) {
+      const int n = nterms[3 * r + s];
+      if (n <= 0) {
+        delete p;
+        return FMM_E_PLAN;
+      }
+      *first[s] = (int)p->terms.size();
+      *count[s] = n;
+      for (int q = 0; q < n; ++q, ++pos) {
+        if (rows[pos] < 0 || rows[pos] >= lim[s][0] || cols[pos] < 0 || cols[pos] >= lim[s][1]) {
+          delete p;
+          return FMM_E_PLAN;
+        }
+        p->terms.push_back(fmm::Term{rows[pos], cols[pos], coefs[pos]});
+      }
+    }
+    p->prods.push_back(pr);
+  }
+  // C block lists for the scatter (products in increasing order per block).
+  const int nblk = dims[0] * dims[2];
+  std::vector<std::vector<std::pair<int, double>>> lists(nblk);
+  for (int r = 0; r < rank; ++r) {
+    const fmm::Prod& pr = p->prods[r];
+    for (int q = 0; q < pr.nc; ++q) {
+      const fmm::Term& t = p->terms[pr.c0 + q];
+      lists[t.row * dims[2] + t.col].push_back({r, t.coef});
+    }
+  }
+  for (int b = 0; b < nblk; ++b) {
+    if (lists[b].empty()) continue;
+    p->cblk.push_back(b / dims[2]);
+    p->cblk.push_back(b % dims[2]);
+    p->cblk.push_back((int)p->ent_r.size());
+    p->cblk.push_back((int)lists[b].size());
+    for (auto& e : lists[b]) {
+      p->ent_r.push_back(e.first);
+      p->ent_w.push_back(e.second);
+    }
+    ++p->n_cblk;
+  }
+  *out = p;
+  return FMM_OK;
+}
+
+fmm_plan* classical_plan() {
+  static fmm_plan* p = [] {
+    const int dims[3] = {1, 1, 1};
+    const int nt[3] = {1, 1, 1};
+    const int rows[3] = {0, 0, 0}, cols[3] = {0, 0, 0};
+    const double coefs[3] = {1.0, 1.0, 1.0};
+    fmm_plan* q = nullptr;
+    build_plan(dims, 1, nt, rows, cols, coefs, &q);
+    return q;
+  }();
+  return p;
+}
+
+bool smem_configured[kMaxDevices];
+std::mutex g_attr_mu;
+
+int configure_kernel() {
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (!smem_configured[dev]) {
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::SMEM_BYTES));
+    smem_configured[dev] = true;
+  }
+  return FMM_OK;
+}
+
+// Launch the DMMA GEMM over sub-blocks of size ms x ks x ns.
+int launch_gemm(const DevTables& d, int r_begin, int r_end, int mode, const double* A, long long lda,
+                const double* B, long long ldb, double* C, long long ldc, double* M, long long ldm,
+                long long m_stride, int ms, int ns, int ks, cudaStream_t st) {
+  if (ms <= 0 || ns <= 0 || ks <= 0 || r_end <= r_begin) return FMM_OK;
+  int rc = configure_kernel();
+  if (rc != FMM_OK) return rc;
+  fmm::GemmArgs a{};
+  a.A = A;
+  a.lda = lda;
+  a.B = B;
+  a.ldb = ldb;
+  a.C = C;
+  a.ldc = ldc;
+  a.M = M;
+  a.ldm = ldm;
+  a.m_stride = m_stride;
+  a.ms = ms;
+  a.ns = ns;
+  a.ks = ks;
+  a.prods = d.prods;
+  a.terms = d.terms;
+  a.r_begin = r_begin;
+  a.r_end = r_end;
+  a.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
+  a.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
+  a.mode = mode;
+  dim3 grid((unsigned)(a.tiles_m * a.tiles_n), mode == fmm::MODE_STORE_M ? (unsigned)(r_end - r_begin) : 1u);
+  fmm::fmm_gemm_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES, st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cuda_status(cudaGetLastError());
+}
+
+int plain_gemm(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, double* C,
+               long long ldc, cudaStream_t st) {
+  if (m <= 0 || n <= 0 || k <= 0) return FMM_OK;
+  DevTables* d = nullptr;
+  int rc = device_tables(classical_plan(), &d);
+  if (rc != FMM_OK) return rc;
+  return launch_gemm(*d, 0, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
+}
+
+int grid_for(long long total, int threads) {
+  long long b = (total + threads - 1) / threads;
+  if (b > 148LL * 16) b = 148LL * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Fringe GEMMs, same regions and order as the reference's dynamic peeling.
+int peel(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, double* C,
+         long long ldc, int dim1, int dim2, int dim3, cudaStream_t st) {
+  const int mr = m % dim1, kr = k % dim2, nr = n % dim3;
+  const int ms = m - mr, ns = n - nr, ks = k - kr;
+  int rc = FMM_OK;
+  if (kr > 0 && ms > 0 && ns > 0) {
+    rc = plain_gemm(ms, ns, kr, A + (long long)ks * lda, lda, B + ks, ldb, C, ldc, st);
+    if (rc != FMM_OK) return rc;
+  }
+  if (nr > 0) {
+    rc = plain_gemm(m, nr, k, A, lda, B + (long long)ns * ldb, ldb, C + (long long)ns * ldc, ldc, st);
+    if (rc != FMM_OK) return rc;
+  }
+  if (mr > 0 && ns > 0) {
+    rc = plain_gemm(mr, ns, k, A + ms, lda, B, ldb, C + ms, ldc, st);
+    if (rc != FMM_OK) return rc;
+  }
+  return FMM_OK;
+}
+
+int check_args(int m, int n, int k, const void* A, long long lda, const void* B, long long ldb, const void* C,
+               long long ldc) {
+  if (m < 0 || n < 0 || k < 0) return FMM_E_INVALID;
+  if (m == 0 || n == 0 || k == 0) return FMM_OK;
+  if (!A || !B || !C) return FMM_E_INVALID;
+  if (lda < m || ldb < k || ldc < m) return FMM_E_INVALID;
+  return FMM_OK;
+}
+
+int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A, long long lda, const double* B,
+            long long ldb, double* C, long long ldc, cudaStream_t st) {
+  if (!plan) return FMM_E_NOPLAN;
+  if (pack != FMM_PACK_ABC && pack != FMM_PACK_AB && pack != FMM_PACK_NAIVE) return FMM_E_UNSUPPORTED;
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK) return rc;
+  if (m == 0 || n == 0 || k == 0) return FMM_OK;
+  const int pm = plan->dims[0] * kMR, pk = plan->dims[1], pn = plan->dims[2] * kNR;
+  const int md = m - m % pm, kd = k - k % pk, nd = n - n % pn;
+  const int ms = md / plan->dims[0], ks = kd / plan->dims[1], ns = nd / plan->dims[2];
+  DevTables* d = nullptr;
+  rc = device_tables(plan, &d);
+  if (rc != FMM_OK) return rc;
+  const int R = plan->rank;
+  if (ms > 0 && ns > 0 && ks > 0) {
+    if (pack == FMM_PACK_ABC) {
+      rc = launch_gemm(*d, 0, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+      if (rc != FMM_OK) return rc;
+    } else {
+      const long long mstride = (long long)ms * ns;
+      size_t bytes = sizeof(double) * (size_t)mstride * R;
+      size_t s_bytes = 0, t_bytes = 0;
+      if (pack == FMM_PACK_NAIVE) {
+        s_bytes = sizeof(double) * (size_t)ms * ks * R;
+        t_bytes = sizeof(double) * (size_t)ks * ns * R;
+      }
+      char* ws = nullptr;
+      FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes + s_bytes + t_bytes, st));
+      double* M = reinterpret_cast<double*>(ws);
+      if (pack == FMM_PACK_AB) {
+        rc = launch_gemm(*d, 0, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
+      } else {
+        double* S = reinterpret_cast<double*>(ws + bytes);
+        double* T = reinterpret_cast<double*>(ws + bytes + s_bytes);
+        fmm::LincombArgs la{};
+        la.X = A;
+        la.ldx = lda;
+        la.rows = ms;
+        la.cols = ks;
+        la.blk_row_stride = ms;
+        la.blk_col_stride = ks;
+        la.out = S;
+        la.ldo = ms;
+        la.out_stride = (long long)ms * ks;
+        la.prods = d->prods;
+        la.terms = d->terms;
+        la.side = 0;
+        la.r_begin = 0;
+        const dim3 ga((unsigned)grid_for((long long)ms * ks, 256), (unsigned)R);
+        fmm::fmm_lincomb_kernel<<<ga, 256, 0, st>>>(la);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        fmm::LincombArgs lb = la;
+        lb.X = B;
+        lb.ldx = ldb;
+        lb.rows = ks;
+        lb.cols = ns;
+        lb.blk_row_stride = ks;
+        lb.blk_col_stride = ns;
+        lb.out = T;
+        lb.ldo = ks;
+        lb.out_stride = (long long)ks * ns;
+        lb.side = 1;
+        const dim3 gb((unsigned)grid_for((long long)ks * ns, 256), (unsigned)R);
+        fmm::fmm_lincomb_kernel<<<gb, 256, 0, st>>>(lb);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        rc = cuda_status(cudaGetLastError());
+        // Product r: M_r = S_r * T_r, with S_r the block (0, r) of an ms x (R*ks) matrix.
+        if (rc == FMM_OK) {
+          DevTables* dc = nullptr;
+          rc = device_tables(classical_plan(), &dc);
+          for (int r = 0; rc == FMM_OK && r < R; ++r) {
+            rc = launch_gemm(*dc, 0, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
+                             T + (long long)r * ks * ns, ks, nullptr, 0, M + (long long)r * mstride, ms, 0, ms, ns,
+                             ks, st);
+          }
+        }
+      }
+      if (rc == FMM_OK) {
+        fmm::ScatterArgs sa{};
+        sa.C = C;
+        sa.ldc = ldc;
+        sa.ms = ms;
+        sa.ns = ns;
+        sa.M = M;
+        sa.ldm = ms;
+        sa.m_stride = mstride;
+        sa.cblk = d->cblk;
+        sa.ent_r = d->ent_r;
+        sa.ent_w = d->ent_w;
+        const dim3 gs((unsigned)grid_for(mstride, 256), (unsigned)plan->n_cblk);
+        fmm::fmm_scatter_kernel<<<gs, 256, 0, st>>>(sa);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        rc = cuda_status(cudaGetLastError());
+      }
+      cudaError_t fe = cudaFreeAsync(ws, st);
+      if (rc == FMM_OK) rc = cuda_status(fe);
+      if (rc != FMM_OK) return rc;
+    }
+  }
+  return peel(m, n, k, A, lda, B, ldb, C, ldc, pm, pk, pn, st);
+}
+
+// Host-pointer execution: stage A, B, C into device memory, run, copy C back.
+int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, const double* A, int lda,
+             const double* B, int ldb, double* C, int ldc) {
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK) return rc;
+  if (m == 0 || n == 0 || k == 0) return FMM_OK;
+  if (!plain && !plan) return FMM_E_NOPLAN;
+  cudaStream_t st = cudaStreamPerThread;
+  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  const size_t szA = sizeof(double) * (size_t)m * k, szB = sizeof(double) * (size_t)k * n,
+               szC = sizeof(double) * (size_t)m * n;
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&dA, szA, st));
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&dB, szB, st));
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&dC, szC, st));
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, sizeof(double) * m, A, sizeof(double) * lda, sizeof(double) * m, k,
+                                 cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, sizeof(double) * k, B, sizeof(double) * ldb, sizeof(double) * k, n,
+                                 cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, sizeof(double) * m, C, sizeof(double) * ldc, sizeof(double) * m, n,
+                                 cudaMemcpyHostToDevice, st));
+  if (plain)
+    rc = plain_gemm(m, n, k, dA, m, dB, k, dC, m, st);
+  else
+    rc = run_fmm(plan, pack, m, n, k, dA, m, dB, k, dC, m, st);
+  if (rc == FMM_OK)
+    rc = cuda_status(cudaMemcpy2DAsync(C, sizeof(double) * ldc, dC, sizeof(double) * m, sizeof(double) * m, n,
+                                       cudaMemcpyDeviceToHost, st));
+  cudaFreeAsync(dA, st);
+  cudaFreeAsync(dB, st);
+  cudaFreeAsync(dC, st);
+  cudaError_t se = cudaStreamSynchronize(st);
+  if (rc == FMM_OK) rc = cuda_status(se);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmm_plan_create(const int dims[3], int rank, const int* nterms, const int* rows, const int* cols,
+                    const double* coefs, fmm_plan** out) {
+  return build_plan(dims, rank, nterms, rows, cols, coefs, out);
+}
+
+int fmm_plan_destroy(fmm_plan* plan) {
+  if (!plan) return FMM_E_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    if (g_default_plan == plan) g_default_plan = nullptr;
+  }
+  for (auto& d : plan->dev) {
+    if (!d.ready) continue;
+    cudaFree(d.prods);
+    cudaFree(d.terms);
+    cudaFree(d.cblk);
+    cudaFree(d.ent_r);
+    cudaFree(d.ent_w);
+  }
+  delete plan;
+  return FMM_OK;
+}
+
+int fmm_plan_rank(const fmm_plan* plan) { return plan ? plan->rank : FMM_E_INVALID; }
+
+int fmm_bind_default_plan(fmm_plan* plan) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  g_default_plan = plan;
+  return FMM_OK;
+}
+
+fmm_plan* fmm_default_plan(void) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  return g_default_plan;
+}
+
+int fmm_dgemm_dev(const fmm_plan* plan, int pack_type, int m, int n, int k, const double* A, long lda,
+                  const double* B, long ldb, double* C, long ldc, void* stream) {
+  return run_fmm(plan, pack_type, m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+}
+
+int fmm_plain_dgemm_dev(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
+                        long ldc, void* stream) {
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK) return rc;
+  return plain_gemm(m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+}
+
+int fmm_dgemm_host(const fmm_plan* plan, int pack_type, int m, int n, int k, const double* A, int lda,
+                   const double* B, int ldb, double* C, int ldc) {
+  return run_host(plan, pack_type, false, m, n, k, A, lda, B, ldb, C, ldc);
+}
+
+void bl_dgemm(int m, int n, int k, double* A, int lda, double* B, int ldb, double* C, int ldc) {
+  t_last_error = run_host(nullptr, 0, true, m, n, k, A, lda, B, ldb, C, ldc);
+}
+
+void bl_dgemm_strassen_abc(int m, int n, int k, double* A, int lda, double* B, int ldb, double* C, int ldc) {
+  t_last_error = run_host(fmm_default_plan(), FMM_PACK_ABC, false, m, n, k, A, lda, B, ldb, C, ldc);
+}
+
+void bl_dgemm_strassen_ab(int m, int n, int k, double* A, int lda, double* B, int ldb, double* C, int ldc) {
+  t_last_error = run_host(fmm_default_plan(), FMM_PACK_AB, false, m, n, k, A, lda, B, ldb, C, ldc);
+}
+
+void bl_dgemm_strassen_naive(int m, int n, int k, double* A, int lda, double* B, int ldb, double* C, int ldc) {
+  t_last_error = run_host(fmm_default_plan(), FMM_PACK_NAIVE, false, m, n, k, A, lda, B, ldb, C, ldc);
+}
+
+void bl_dynamic_peeling(int m, int n, int k, double* A, int lda, double* B, int ldb, double* C, int ldc, int dim1,
+                        int dim2, int dim3) {
+  if (dim1 <= 0 || dim2 <= 0 || dim3 <= 0) {
+    t_last_error = FMM_E_INVALID;
+    return;
+  }
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK || m == 0 || n == 0 || k == 0) {
+    t_last_error = rc;
+    return;
+  }
+  cudaStream_t st = cudaStreamPerThread;
+  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  const size_t szA = sizeof(double) * (size_t)m * k, szB = sizeof(double) * (size_t)k * n,
+               szC = sizeof(double) * (size_t)m * n;
+  rc = cuda_status(cudaMallocAsync((void**)&dA, szA, st));
+  if (rc == FMM_OK) rc = cuda_status(cudaMallocAsync((void**)&dB, szB, st));
+  if (rc == FMM_OK) rc = cuda_status(cudaMallocAsync((void**)&dC, szC, st));
+  if (rc == FMM_OK)
+    rc = cuda_status(cudaMemcpy2DAsync(dA, sizeof(double) * m, A, sizeof(double) * lda, sizeof(double) * m, k,
+                                       cudaMemcpyHostToDevice, st));
+  if (rc == FMM_OK)
+    rc = cuda_status(cudaMemcpy2DAsync(dB, sizeof(double) * k, B, sizeof(double) * ldb, sizeof(double) * k, n,
+                                       cudaMemcpyHostToDevice, st));
+  if (rc == FMM_OK)
+    rc = cuda_status(cudaMemcpy2DAsync(dC, sizeof(double) * m, C, sizeof(double) * ldc, sizeof(double) * m, n,
+                                       cudaMemcpyHostToDevice, st));
+  if (rc == FMM_OK) rc = peel(m, n, k, dA, m, dB, k, dC, m, dim1, dim2, dim3, st);
+  if (rc == FMM_OK)
+    rc = cuda_status(cudaMemcpy2DAsync(C, sizeof(double) * ldc, dC, sizeof(double) * m, sizeof(double) * m, n,
+                                       cudaMemcpyDeviceToHost, st));
+  if (dA) cudaFreeAsync(dA, st);
+  if (dB) cudaFreeAsync(dB, st);
+  if (dC) cudaFreeAsync(dC, st);
+  cudaError_t se = cudaStreamSynchronize(st);
+  if (rc == FMM_OK) rc = cuda_status(se);
+  t_last_error = rc;
+}
+
+int fmm_last_error(void) { return t_last_error; }
+
+const char* fmm_error_string(int code) {
+  switch (code) {
+    case FMM_OK: return "ok";
+    case FMM_E_INVALID: return "invalid argument (dimension, leading dimension or pointer)";
+    case FMM_E_NOPLAN: return "no FMM plan bound";
+    case FMM_E_CUDA: return "CUDA runtime error";
+    case FMM_E_NOMEM: return "out of memory";
+    case FMM_E_PLAN: return "malformed plan tables";
+    case FMM_E_UNSUPPORTED: return "unsupported pack type or option";
+    case FMM_E_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown error";
+  }
+}
+
+long long fmm_kernel_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+/*
+ * fmm_b200 — B200-native (sm_100a) generated fast matrix multiplication, C ABI.
+ *
+ * Semantics match the reference's generated entry points: column-major FP64,
+ * C += A * B (alpha = beta = 1, no transposes).  Unlike the reference, C needs no
+ * padding or alignment: any ldc >= m works.
+ *
+ * Two families of entry points:
+ *   1. Drop-in symbols with the reference's exact signatures (host pointers,
+ *      synchronous).  They run the plan bound with fmm_bind_default_plan(); a job
+ *      library written by the generator (fmm_gen_b200.control) binds its plan when
+ *      it is loaded, so one job library per algorithm configuration, as in the
+ *      reference.
+ *   2. Stream-ordered device-pointer entry points with status codes (the form a
+ *      PyTorch custom op or another GPU library binds).
+ *
+ * Every function that returns int returns FMM_OK (0) or a negative FMM_E* code;
+ * fmm_error_string() names it.  The void drop-in symbols record their status in
+ * fmm_last_error().
+ */
+#ifndef FMM_B200_H
+#define FMM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMM_OK 0
+#define FMM_E_INVALID (-1)      /* bad dimension, leading dimension or pointer */
+#define FMM_E_NOPLAN (-2)       /* no default plan bound */
+#define FMM_E_CUDA (-3)         /* a CUDA runtime call failed */
+#define FMM_E_NOMEM (-4)        /* device or host allocation failed */
+#define FMM_E_PLAN (-5)         /* malformed plan tables */
+#define FMM_E_UNSUPPORTED (-6)  /* pack type or option not supported */
+#define FMM_E_TIMEOUT (-7)      /* a bounded device-side wait gave up */
+
+#define FMM_PACK_ABC 0    /* sums fused into operand staging, products scattered into C */
+#define FMM_PACK_AB 1     /* sums fused into staging, each product to a workspace M_r, then scatter */
+#define FMM_PACK_NAIVE 2  /* explicit S_r, T_r temporaries, plain GEMM into M_r, then scatter */
+
+typedef struct fmm_plan fmm_plan;
+
+/* ---- drop-in symbols (reference: common/include/bl_dgemm.h:60-70, 96-130) ---- */
+
+/* Classical C += A*B (reference bl_dgemm, common/dgemm/my_dgemm.c:115-210). */
+void bl_dgemm(int m, int n, int k, double *A, int lda, double *B, int ldb, double *C, int ldc);
+
+/* Generated FMM entry points (reference bl_dgemm_strassen_abc/_ab/_naive, emitted by
+ * meta/abc_gen_mix.py:448-472, meta/ab_gen_mix.py:430-456, meta/naive_gen_mix.py:412-429).
+ * They run the default plan. */
+void bl_dgemm_strassen_abc(int m, int n, int k, double *A, int lda, double *B, int ldb, double *C, int ldc);
+void bl_dgemm_strassen_ab(int m, int n, int k, double *A, int lda, double *B, int ldb, double *C, int ldc);
+void bl_dgemm_strassen_naive(int m, int n, int k, double *A, int lda, double *B, int ldb, double *C, int ldc);
+
+/* Fringe GEMMs around the FMM core (reference bl_dynamic_peeling,
+ * common/dgemm/bl_dgemm_util.c:316-353); host pointers. */
+void bl_dynamic_peeling(int m, int n, int k, double *A, int lda, double *B, int ldb, double *C, int ldc,
+                        int dim1, int dim2, int dim3);
+
+/* Status of the last drop-in call on this host thread. */
+int fmm_last_error(void);
+const char *fmm_error_string(int code);
+
+/* ---- plans ---- */
+
+/* Create a plan from composed term lists (the generator's output).
+ *   dims[3]       = (prod mt, prod kt, prod nt) over all levels
+ *   rank          = number of products R
+ *   nterms[3*R]   = per product r: #A terms, #B terms, #C terms
+ *   rows, cols, coefs: the terms, product-major, A terms then B then C per product;
+ *                   (row, col) is the global block position in the composed grid.
+ * Replaces the reference's per-configuration generated code (meta/abc_gen_mix.py:407-472). */
+int fmm_plan_create(const int dims[3], int rank, const int *nterms, const int *rows, const int *cols,
+                    const double *coefs, fmm_plan **out);
+int fmm_plan_destroy(fmm_plan *plan);
+int fmm_plan_rank(const fmm_plan *plan);
+int fmm_bind_default_plan(fmm_plan *plan);
+fmm_plan *fmm_default_plan(void);
+
+/* ---- stream-ordered device entry points ---- */
+
+/* FMM C += A*B on device pointers, enqueued on `stream` (a cudaStream_t; NULL = legacy
+ * default stream).  Workspace for AB/NAIVE comes from the stream-ordered allocator. */
+int fmm_dgemm_dev(const fmm_plan *plan, int pack_type, int m, int n, int k, const double *A, long lda,
+                  const double *B, long ldb, double *C, long ldc, void *stream);
+
+/* Classical C += A*B on device pointers (the comparator and fringe engine). */
+int fmm_plain_dgemm_dev(int m, int n, int k, const double *A, long lda, const double *B, long ldb, double *C,
+                        long ldc, void *stream);
+
+/* Host-pointer FMM with an explicit plan: copies A, B, C to the device, runs, copies C
+ * back, synchronises.  The drop-in symbols above call this with the default plan. */
+int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, const double *A, int lda,
+                   const double *B, int ldb, double *C, int ldc);
+
+/* Number of kernels the library launched since load (all entry points, all streams). */
+long long fmm_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMM_B200_H */
