@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the generated FMM GEMM on B200: effective TFLOPS = 2mnk/t.
+
+Workload (one step): the two-level hybrid 222-1 x 333-1 (Strassen x Smirnov <3,3,3;23>),
+pack type abc, FP64 column-major C += A*B on the three shapes of that configuration:
+16384^3, 14400x14400x480 (rank-k) and 4000x16000x2000, with A, B, C ~ U(-1,1) from a
+seed.  Inputs stay resident in HBM; every step touches ~8.5 GB, far more than the
+126 MB L2, so no extra L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Under torchrun (N > 1) every rank runs the same workload on
+its own inputs (independent replicas: a single GEMM is not split across GPUs), and the
+value is the sum over ranks divided by the slowest rank's device time.
+`--impl reference` times the CPU restatement of the reference's algorithm (the oracle)
+on the host cores instead, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALGS, LEVELS, PACK = ["222", "333"], [1, 1], "abc"
+SHAPES = [(16384, 16384, 16384), (14400, 14400, 480), (4000, 16000, 2000)]
+WORKLOAD = "222-1x333-1 abc FP64 C+=A*B over 16384^3, 14400x14400x480, 4000x16000x2000"
+METRIC = "effective TFLOPS (2mnk/t), 222-1x333-1 abc FP64"
+UNIT = "TFLOP/s"
+CPU_SAMPLE = (14400, 14400, 480)
+# DRAM traffic of one fmm_gemm_kernel launch per unit of work, from the ncu capture
+# summarised in profiles/ (bytes per executed core flop); None until captured.
+TRAFFIC_BYTES_PER_FLOP = None
+
+
+def effective_flops(shapes):
+    return sum(2.0 * m * n * k for (m, n, k) in shapes)
+
+
+def core_flops(plan, shapes):
+    from fmm_gen_b200 import algebra
+
+    tot = 0.0
+    for (m, n, k) in shapes:
+        p = algebra.partition(m, n, k, plan.dims)
+        tot += plan.rank * 2.0 * p.ms * p.ns * p.ks
+    return tot
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            with open(self.path) as fh:
+                for r in csv.reader(fh):
+                    if len(r) >= 9:
+                        rows.append([x.strip() for x in r])
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
+        power = [num(r[3]) for r in rows if num(r[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+def oracle_sample_tflops(shape, reps=1):
+    """CPU restatement of the reference's abc algorithm (the oracle) on the host cores."""
+    import numpy as np
+
+    from fmm_gen_b200 import algebra, runtime
+    from oracle import cpu
+
+    plan = algebra.make_plan(ALGS, LEVELS)
+    dims, nterms, rows, cols, coefs = runtime.plan_tables(plan)
+    tables = (dims, plan.rank, nterms, rows, cols, coefs)
+    m, n, k = shape
+    rng = np.random.default_rng(99)
+    A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        cpu.fmm(tables, PACK, A, B, C)
+        times.append(time.perf_counter() - t0)
+    return 2.0 * m * n * k / min(times) / 1e12, cpu.num_threads(), times
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU restatement of the reference's algorithm, timed on the host."""
+    if rank != 0:
+        return
+    sample = CPU_SAMPLE
+    for _ in range(args.warmup):
+        oracle_sample_tflops(sample)
+    t0 = time.perf_counter()
+    per = []
+    for _ in range(args.steps):
+        v, cores, ts = oracle_sample_tflops(sample)
+        per.append(ts[0])
+    total = time.perf_counter() - t0
+    m, n, k = sample
+    value = 2.0 * m * n * k * args.steps / total / 1e12
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_shape": list(sample), "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"one 222-1x333-1 abc C+=A*B at {m}x{n}x{k} (the workload's rank-k shape) "
+                                   "per step, oracle/fmm_oracle.c with OpenMP"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    from fmm_gen_b200 import algebra, runtime as rt
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_
+
+        dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_
+    dev = torch.device("cuda", local)
+    plan = rt.Plan.from_levels(ALGS, LEVELS)
+    g = torch.Generator(device=dev).manual_seed(1000 + rank)
+    mats = []
+    for (m, n, k) in SHAPES:
+        A = rt.colmajor(m, k, device=dev).uniform_(-1, 1, generator=g)
+        B = rt.colmajor(k, n, device=dev).uniform_(-1, 1, generator=g)
+        C = rt.colmajor(m, n, device=dev).uniform_(-1, 1, generator=g)
+        mats.append((A, B, C))
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        for (A, B, C) in mats:
+            rt.fmm_gemm(plan, A, B, C, PACK, stream=stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- timed region ----
+    launches0 = rt.kernel_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with rt.KernelTimer() as kt:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+    barrier()
+    launches = rt.kernel_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    eff = effective_flops(SHAPES)
+    value = world * eff * args.steps / (ms_max * 1e-3) / 1e12
+    clk = clocks.summary()
+
+    # ---- dominant kernel roofline (FP64 DMMA bound) ----
+    core_name = "fmm_gemm_kernel[fmm products]"
+    core_ms = kt.ms[core_name]
+    core_launches = kt.count[core_name]
+    cflops = core_flops(plan.algebra, SHAPES) * args.steps
+    achieved = cflops / (core_ms * 1e-3) / 1e12 if core_ms > 0 else None
+
+    # measured FP64 tensor peak: cuBLAS DGEMM 8192^3 on this GPU, this run
+    a = torch.rand(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.rand(8192, 8192, dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        torch.matmul(a, b, out=c)
+        s1.record()
+        torch.cuda.synchronize()
+        best = min(best, s0.elapsed_time(s1))
+    peak = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del a, b, c
+
+    # ---- correctness of this run's result against a classical FP64 GEMM ----
+    errs = {}
+    for (m, n, k), (A, B, C) in zip(SHAPES, mats):
+        C0 = rt.colmajor(m, n, device=dev).copy_(C)
+        ref = torch.addmm(C0, A, B)
+        rt.fmm_gemm(plan, A, B, C0, PACK)
+        errs[f"{m}x{n}x{k}"] = ((C0 - ref).norm() / ref.norm()).item()
+        del C0, ref
+    torch.cuda.empty_cache()
+
+    # ---- comparators: the project's plain FP64 GEMM, and 222-1 at 16384^3 ----
+    def time_call(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            fn()
+        s1.record()
+        torch.cuda.synchronize()
+        return s0.elapsed_time(s1) / reps
+
+    plain_ms = sum(time_call(lambda A=A, B=B, C=C: rt.plain_gemm(A, B, C)) for (A, B, C) in mats)
+    plain_tflops = eff / (plain_ms * 1e-3) / 1e12
+    A16, B16, C16 = mats[0]
+    p1 = rt.Plan.from_levels(["222"], [1])
+    s222 = time_call(lambda: rt.fmm_gemm(p1, A16, B16, C16, "abc"))
+    s_plain16 = time_call(lambda: rt.plain_gemm(A16, B16, C16))
+    f16 = 2.0 * 16384 ** 3
+
+    # ---- end to end through the host C ABI (pinned host buffers, copies in the timed region) ----
+    host = []
+    for (A, B, C) in mats:
+        hs = []
+        for X in (A, B, C):
+            h = torch.empty(X.shape[1], X.shape[0], dtype=torch.float64, pin_memory=True).t()
+            h.copy_(X)
+            hs.append(h.numpy())
+        host.append(hs)
+    h2d = sum(8 * (m * k + k * n + m * n) for (m, n, k) in SHAPES)
+    d2h = sum(8 * m * n for (m, n, k) in SHAPES)
+    for (hA, hB, hC) in host:  # warm the host path (workspace pool)
+        rt.fmm_gemm_host(plan, hA, hB, hC, PACK)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for (hA, hB, hC) in host:
+            rt.fmm_gemm_host(plan, hA, hB, hC, PACK)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * eff * args.steps / float(te.item()) / 1e12
+    del host
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, ts = oracle_sample_tflops(CPU_SAMPLE)
+        cpu_baseline = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                        "sample": f"one 222-1x333-1 abc C+=A*B at {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} "
+                                  f"(the workload's rank-k shape), oracle/fmm_oracle.c with OpenMP, {ts[0]:.1f} s"}
+
+    if rank == 0:
+        per_launch_flops = cflops / max(core_launches, 1)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "algorithm": "222-1_333-1", "pack_type": PACK,
+                       "shapes": [list(s) for s in SHAPES], "inputs": "A,B,C ~ U(-1,1), seeded",
+                       "l2": "inputs larger than L2 (8.5 GB per step), no flush",
+                       "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "fmm_dgemm_host (C ABI, pinned host buffers)"},
+            "roofline": {"bound": "tensor", "kernel": core_name, "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                         "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU in this run (FP64 tensor)",
+                         "traffic": (TRAFFIC_BYTES_PER_FLOP * per_launch_flops) if TRAFFIC_BYTES_PER_FLOP else None,
+                         "launches": core_launches, "avg_launch_ms": core_ms / max(core_launches, 1),
+                         "executed_flops_per_launch": per_launch_flops},
+            "kernel_ms": kt.ms, "kernel_launches": kt.count,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu_baseline,
+            "plain_fp64": {"tflops": plain_tflops, "fmm_over_plain": value / world / plain_tflops},
+            "strassen_222_1_16384": {"fmm_tflops": f16 / (s222 * 1e-3) / 1e12,
+                                     "plain_tflops": f16 / (s_plain16 * 1e-3) / 1e12,
+                                     "ratio": s_plain16 / s222},
+            "rel_fro_err_vs_cublas": errs,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

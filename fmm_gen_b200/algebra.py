@@ -395,20 +395,42 @@ def executed_flops(plan: FMMPlan, m: int, n: int, k: int) -> float:
     return core + fringe
 
 
-def stability_emax(plan: FMMPlan) -> float:
-    """Norm-wise error growth factor of a (composed) FMM.
+def e_max(plan: FMMPlan) -> float:
+    """Largest coefficient-weighted product count feeding one C block:
 
-    Follows the stability analysis of Ballard, Benson, Druinsky, Lipshitz and Schwartz
-    ("Improving the numerical stability of fast matrix multiplication", SIMAX 2016):
-    with alpha = max_r nnz(U[:,r]) style quantities the forward error of one level is
-    bounded by (alpha + beta + gamma) * e_max * u * ||A|| ||B||, where e_max is the
-    largest number of nonzero products feeding one output entry weighted by the
-    coefficient magnitudes.  The multi-level bound is the product of per-level terms.
-    Returned value is a multiplicative factor on k * u * ||A||_max ||B||_max.
+        e_max = max_l sum_r |W[l,r]| * ||U[:,r]||_1 * ||V[:,r]||_1
+
+    (12 for Strassen).  It is multiplicative under the Kronecker composition, so the
+    composed plan's value equals the product of the levels' values.  This quantity
+    appears in the stability analysis of fast matrix multiplication by Ballard,
+    Benson, Druinsky, Lipshitz and Schwartz (SIMAX 37(4), 2016).
     """
-    U, V, W = plan.U, plan.V, plan.W
-    a = np.abs(U).sum(axis=0)  # per product: |U| column sums
-    b = np.abs(V).sum(axis=0)
-    # e_max: for each output block l, sum over products of |W[l,r]| * a_r * b_r
-    e = (np.abs(W) * (a * b)[None, :]).sum(axis=1)
-    return float(e.max())
+    a = np.abs(plan.U).sum(axis=0)
+    b = np.abs(plan.V).sum(axis=0)
+    return float((np.abs(plan.W) * (a * b)[None, :]).sum(axis=1).max())
+
+
+def error_bound(plan: FMMPlan, m: int, n: int, k: int, amax: float, bmax: float, cmax: float = 0.0,
+                unit_roundoff: float = 2.0 ** -53) -> float:
+    """First-order max-norm forward error bound of one FMM call C += A*B.
+
+    Derivation (elementwise, standard rounding-error analysis): an operand sum with
+    at most `a` terms is off by <= a*u*sum|u_i||A_i|; a product of depth K_s adds
+    K_s*u*|S||T|; accumulating the products into a C block with at most `c` terms adds
+    c*u*(|C| + sum_r |w||M_r|).  With |S_r| <= ||U[:,r]||_1 ||A||_max and likewise for
+    T_r this gives
+
+        |C_hat - C|_max <= (a + b + c + K_s) u K_s e_max ||A||_max ||B||_max + (c+1) u ||C0||_max
+
+    and the classical fringe GEMMs satisfy the same form with e_max = 1, depth k.
+    The bound holds for any summation order, so it covers both the reference's
+    KC-chunked CPU arithmetic and the GPU's fused multiply-adds.
+    """
+    p = partition(m, n, k, plan.dims)
+    ta, tb, tc = plan.max_terms
+    ks = max(p.ks, 1)
+    core = (ta + tb + tc + ks) * ks * e_max(plan)
+    fringe = (k + 2) * k
+    if p.kr > 0:
+        core += (p.kr + 2) * p.kr
+    return unit_roundoff * (max(core, fringe) * amax * bmax + (tc + 2) * cmax)

@@ -29,6 +29,40 @@ constexpr int kNR = 4;
 std::atomic<long long> g_launches{0};
 thread_local int t_last_error = FMM_OK;
 
+// Optional per-kernel timing: when enabled, every launch is bracketed by CUDA events on
+// its own stream; fmm_profile_end() sums the durations per kernel kind.
+enum KernelKind { K_GEMM_FMM = 0, K_GEMM_CLASSICAL = 1, K_LINCOMB = 2, K_SCATTER = 3, K_NUM = 4 };
+const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
+                                         "fmm_lincomb_kernel", "fmm_scatter_kernel"};
+struct ProfRec {
+  int kind;
+  cudaEvent_t e0, e1;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+
+struct ProfScope {
+  int kind;
+  cudaStream_t st;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ProfScope(int k, cudaStream_t s) : kind(k), st(s) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_on) return;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      e0 = e1 = nullptr;
+      return;
+    }
+    cudaEventRecord(e0, st);
+  }
+  ~ProfScope() {
+    if (!e0) return;
+    cudaEventRecord(e1, st);
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof.push_back(ProfRec{kind, e0, e1});
+  }
+};
+
 struct DevTables {
   fmm::Prod* prods = nullptr;
   fmm::Term* terms = nullptr;
@@ -193,7 +227,7 @@ int configure_kernel() {
 }
 
 // Launch the DMMA GEMM over sub-blocks of size ms x ks x ns.
-int launch_gemm(const DevTables& d, int r_begin, int r_end, int mode, const double* A, long long lda,
+int launch_gemm(int kind, const DevTables& d, int r_begin, int r_end, int mode, const double* A, long long lda,
                 const double* B, long long ldb, double* C, long long ldc, double* M, long long ldm,
                 long long m_stride, int ms, int ns, int ks, cudaStream_t st) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || r_end <= r_begin) return FMM_OK;
@@ -220,6 +254,7 @@ int launch_gemm(const DevTables& d, int r_begin, int r_end, int mode, const doub
   a.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
   a.mode = mode;
   dim3 grid((unsigned)(a.tiles_m * a.tiles_n), mode == fmm::MODE_STORE_M ? (unsigned)(r_end - r_begin) : 1u);
+  ProfScope ps(kind, st);
   fmm::fmm_gemm_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES, st>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cuda_status(cudaGetLastError());
@@ -231,7 +266,7 @@ int plain_gemm(int m, int n, int k, const double* A, long long lda, const double
   DevTables* d = nullptr;
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
-  return launch_gemm(*d, 0, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
+  return launch_gemm(K_GEMM_CLASSICAL, *d, 0, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
 }
 
 int grid_for(long long total, int threads) {
@@ -287,7 +322,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   const int R = plan->rank;
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
-      rc = launch_gemm(*d, 0, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+      rc = launch_gemm(K_GEMM_FMM, *d, 0, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
       if (rc != FMM_OK) return rc;
     } else {
       const long long mstride = (long long)ms * ns;
@@ -301,7 +336,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
       FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes + s_bytes + t_bytes, st));
       double* M = reinterpret_cast<double*>(ws);
       if (pack == FMM_PACK_AB) {
-        rc = launch_gemm(*d, 0, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
+        rc = launch_gemm(K_GEMM_FMM, *d, 0, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
       } else {
         double* S = reinterpret_cast<double*>(ws + bytes);
         double* T = reinterpret_cast<double*>(ws + bytes + s_bytes);
@@ -320,7 +355,10 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         la.side = 0;
         la.r_begin = 0;
         const dim3 ga((unsigned)grid_for((long long)ms * ks, 256), (unsigned)R);
-        fmm::fmm_lincomb_kernel<<<ga, 256, 0, st>>>(la);
+        {
+          ProfScope ps(K_LINCOMB, st);
+          fmm::fmm_lincomb_kernel<<<ga, 256, 0, st>>>(la);
+        }
         g_launches.fetch_add(1, std::memory_order_relaxed);
         fmm::LincombArgs lb = la;
         lb.X = B;
@@ -334,7 +372,10 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         lb.out_stride = (long long)ks * ns;
         lb.side = 1;
         const dim3 gb((unsigned)grid_for((long long)ks * ns, 256), (unsigned)R);
-        fmm::fmm_lincomb_kernel<<<gb, 256, 0, st>>>(lb);
+        {
+          ProfScope ps(K_LINCOMB, st);
+          fmm::fmm_lincomb_kernel<<<gb, 256, 0, st>>>(lb);
+        }
         g_launches.fetch_add(1, std::memory_order_relaxed);
         rc = cuda_status(cudaGetLastError());
         // Product r: M_r = S_r * T_r, with S_r the block (0, r) of an ms x (R*ks) matrix.
@@ -342,7 +383,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
           DevTables* dc = nullptr;
           rc = device_tables(classical_plan(), &dc);
           for (int r = 0; rc == FMM_OK && r < R; ++r) {
-            rc = launch_gemm(*dc, 0, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
+            rc = launch_gemm(K_GEMM_FMM, *dc, 0, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
                              T + (long long)r * ks * ns, ks, nullptr, 0, M + (long long)r * mstride, ms, 0, ms, ns,
                              ks, st);
           }
@@ -361,7 +402,10 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         sa.ent_r = d->ent_r;
         sa.ent_w = d->ent_w;
         const dim3 gs((unsigned)grid_for(mstride, 256), (unsigned)plan->n_cblk);
-        fmm::fmm_scatter_kernel<<<gs, 256, 0, st>>>(sa);
+        {
+          ProfScope ps(K_SCATTER, st);
+          fmm::fmm_scatter_kernel<<<gs, 256, 0, st>>>(sa);
+        }
         g_launches.fetch_add(1, std::memory_order_relaxed);
         rc = cuda_status(cudaGetLastError());
       }
@@ -537,5 +581,45 @@ const char* fmm_error_string(int code) {
 }
 
 long long fmm_kernel_launch_count(void) { return g_launches.load(); }
+
+int fmm_profile_begin(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof) {
+    cudaEventDestroy(r.e0);
+    cudaEventDestroy(r.e1);
+  }
+  g_prof.clear();
+  g_prof_on = true;
+  return FMM_OK;
+}
+
+int fmm_profile_end(double* ms_out, long long* count_out) {
+  std::vector<ProfRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_on = false;
+    recs.swap(g_prof);
+  }
+  for (int k = 0; k < K_NUM; ++k) {
+    if (ms_out) ms_out[k] = 0.0;
+    if (count_out) count_out[k] = 0;
+  }
+  int rc = FMM_OK;
+  for (auto& r : recs) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(r.e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, r.e0, r.e1);
+    if (e != cudaSuccess) rc = cuda_status(e);
+    if (ms_out) ms_out[r.kind] += ms;
+    if (count_out) count_out[r.kind] += 1;
+    cudaEventDestroy(r.e0);
+    cudaEventDestroy(r.e1);
+  }
+  return rc;
+}
+
+int fmm_profile_num_kinds(void) { return K_NUM; }
+
+const char* fmm_profile_kind_name(int kind) { return (kind >= 0 && kind < K_NUM) ? kKernelNames[kind] : ""; }
 
 }  // extern "C"

@@ -97,6 +97,14 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_error_string.restype = ctypes.c_char_p
     lib.fmm_kernel_launch_count.argtypes = []
     lib.fmm_kernel_launch_count.restype = ctypes.c_longlong
+    lib.fmm_profile_begin.argtypes = []
+    lib.fmm_profile_begin.restype = c_int
+    lib.fmm_profile_end.argtypes = [c_double_p, ctypes.POINTER(ctypes.c_longlong)]
+    lib.fmm_profile_end.restype = c_int
+    lib.fmm_profile_num_kinds.argtypes = []
+    lib.fmm_profile_num_kinds.restype = c_int
+    lib.fmm_profile_kind_name.argtypes = [c_int]
+    lib.fmm_profile_kind_name.restype = ctypes.c_char_p
 
 
 def _check(rc: int, what: str) -> None:
@@ -244,3 +252,25 @@ def bl_dgemm_host(A: np.ndarray, B: np.ndarray, C: np.ndarray) -> None:
 
 def kernel_launch_count() -> int:
     return int(load_library().fmm_kernel_launch_count())
+
+
+class KernelTimer:
+    """Per-kernel CUDA-event timing of every library launch inside the `with` block.
+
+    After exit, `.ms[name]` and `.count[name]` hold the summed device time and the
+    number of launches per kernel kind."""
+
+    def __enter__(self):
+        self._lib = load_library()
+        _check(self._lib.fmm_profile_begin(), "fmm_profile_begin")
+        return self
+
+    def __exit__(self, *exc):
+        n = self._lib.fmm_profile_num_kinds()
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        _check(self._lib.fmm_profile_end(ms, cnt), "fmm_profile_end")
+        names = [self._lib.fmm_profile_kind_name(i).decode() for i in range(n)]
+        self.ms = {names[i]: ms[i] for i in range(n)}
+        self.count = {names[i]: int(cnt[i]) for i in range(n)}
+        return False

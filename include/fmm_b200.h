@@ -98,6 +98,16 @@ int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, con
 /* Number of kernels the library launched since load (all entry points, all streams). */
 long long fmm_kernel_launch_count(void);
 
+/* Per-kernel timing (no counterpart in the reference, which only times whole calls with
+ * bl_clock, common/dgemm/bl_dgemm_util.c:106-182).  Between begin and end every launch
+ * is bracketed by CUDA events on its stream; end() synchronises those events and
+ * writes, per kernel kind (0 .. fmm_profile_num_kinds()-1), the summed milliseconds and
+ * launch counts. */
+int fmm_profile_begin(void);
+int fmm_profile_end(double *ms_out, long long *count_out);
+int fmm_profile_num_kinds(void);
+const char *fmm_profile_kind_name(int kind);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,110 @@
+"""ORACLE — test infrastructure only.  ctypes wrapper of liboracle.so (fmm_oracle.c),
+the bit-exact CPU restatement of fmm-gen's arithmetic, and of the reference's own
+classical runtime when it was compiled into _ref/ (Makefile target `ref`).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libblislab_ref.so")
+PACKS = {"abc": 0, "ab": 1, "naive": 2}
+
+_lib = None
+_ref = None
+
+
+def build(ref: bool = False) -> None:
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.oracle_bl_dgemm.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci]
+        L.oracle_fmm.argtypes = [ci, vp, ci, vp, vp, vp, vp, ci, ci, ci, vp, ci, vp, ci, vp, ci]
+        L.oracle_dgemm_dot2.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci]
+        L.oracle_dynamic_peeling.argtypes = [ci, ci, ci, vp, ci, vp, ci, vp, ci, ci, ci, ci]
+        L.oracle_num_threads.argtypes = []
+        _lib = L
+    return _lib
+
+
+def load_ref():
+    """The reference's classical runtime (bl_dgemm), or None when it was not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        L = ctypes.CDLL(REF_LIB)
+        L.bl_dgemm.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_int] * 3
+        L.bl_dgemm.restype = None
+        _ref = L
+    return _ref
+
+
+def _cm(x: np.ndarray) -> np.ndarray:
+    if x.dtype != np.float64 or not x.flags.f_contiguous:
+        raise ValueError("oracle arrays must be float64 Fortran-ordered")
+    return x
+
+
+def _p(x):
+    return x.ctypes.data_as(ctypes.c_void_p)
+
+
+def bl_dgemm(A, B, C) -> None:
+    """C += A @ B with the reference's per-element arithmetic (in place, Fortran arrays)."""
+    m, k = A.shape
+    n = B.shape[1]
+    load().oracle_bl_dgemm(m, n, k, _p(_cm(A)), max(m, 1), _p(_cm(B)), max(k, 1), _p(_cm(C)), max(m, 1))
+
+
+def fmm(tables, pack: str, A, B, C) -> None:
+    """FMM C += A @ B; `tables` = (dims, R, nterms, rows, cols, coefs) as int32/float64 arrays."""
+    dims, R, nterms, rows, cols, coefs = tables
+    m, k = A.shape
+    n = B.shape[1]
+    rc = load().oracle_fmm(PACKS[pack], _p(dims), int(R), _p(nterms), _p(rows), _p(cols), _p(coefs), m, n, k,
+                           _p(_cm(A)), max(m, 1), _p(_cm(B)), max(k, 1), _p(_cm(C)), max(m, 1))
+    if rc:
+        raise RuntimeError(f"oracle_fmm failed: {rc}")
+
+
+def dgemm_dot2(A, B, C) -> None:
+    """C += A @ B with compensated (Dot2) dot products: the accuracy reference."""
+    m, k = A.shape
+    n = B.shape[1]
+    load().oracle_dgemm_dot2(m, n, k, _p(_cm(A)), max(m, 1), _p(_cm(B)), max(k, 1), _p(_cm(C)), max(m, 1))
+
+
+def ref_bl_dgemm(A, B, C) -> bool:
+    """The reference's own bl_dgemm (needs a padded, 32 B aligned C; done here).  False if absent."""
+    L = load_ref()
+    if L is None:
+        return False
+    m, k = A.shape
+    n = B.shape[1]
+    ldc = ((m - 1) // 8 + 1) * 8
+    buf = np.zeros(ldc * (n + 4) + 8)
+    off = (-buf.ctypes.data % 32) // 8
+    flat = buf[off:off + ldc * (n + 4)]
+    Cv = flat[: ldc * n].reshape(n, ldc).T
+    Cv[:m, :] = C
+    L.bl_dgemm(m, n, k, _p(_cm(A)), m, _p(_cm(B)), k, flat.ctypes.data_as(ctypes.c_void_p), ldc)
+    C[:, :] = Cv[:m, :n]
+    return True
+
+
+def num_threads() -> int:
+    return int(load().oracle_num_threads())
