@@ -28,6 +28,9 @@
  * accuracy oracle for relative Frobenius errors.
  */
 #include <math.h>
+#ifdef __AVX__
+#include <immintrin.h>
+#endif
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -106,34 +109,62 @@ static void pack_cols(const opnd_t *B, int n, int pc, int pb, double *out) {
   }
 }
 
+/* The 8x4 register tile of one KC chunk: acc(ii,jj) = sum_p a(ii,p)*b(p,jj), each step
+ * a multiply then an add (both rounded), p in order from 0 -- the operation sequence of
+ * the reference's AVX micro-kernel (common/kernels/bl_dgemm_asm_8x4.c:59-300). */
+static inline void micro_8x4(int pb, const double *a, const double *b, double acc[NR][MR]) {
+#ifdef __AVX__
+  __m256d c[NR][2];
+  for (int jj = 0; jj < NR; ++jj) c[jj][0] = c[jj][1] = _mm256_setzero_pd();
+  for (int p = 0; p < pb; ++p) {
+    const __m256d a0 = _mm256_loadu_pd(a + p * MR), a1 = _mm256_loadu_pd(a + p * MR + 4);
+    for (int jj = 0; jj < NR; ++jj) {
+      const __m256d bv = _mm256_broadcast_sd(b + p * NR + jj);
+      c[jj][0] = _mm256_add_pd(c[jj][0], _mm256_mul_pd(a0, bv));
+      c[jj][1] = _mm256_add_pd(c[jj][1], _mm256_mul_pd(a1, bv));
+    }
+  }
+  for (int jj = 0; jj < NR; ++jj) {
+    _mm256_storeu_pd(acc[jj], c[jj][0]);
+    _mm256_storeu_pd(acc[jj] + 4, c[jj][1]);
+  }
+#else
+  for (int jj = 0; jj < NR; ++jj)
+    for (int ii = 0; ii < MR; ++ii) acc[jj][ii] = 0.0;
+  for (int p = 0; p < pb; ++p)
+    for (int jj = 0; jj < NR; ++jj) {
+      const double bv = b[p * NR + jj];
+      for (int ii = 0; ii < MR; ++ii) acc[jj][ii] = acc[jj][ii] + a[p * MR + ii] * bv;
+    }
+#endif
+}
+
 /* One KC chunk: for every element acc = sum_p a*b (in p order, from 0), then each
- * destination d: D_d(i,j) = upd(D_d(i,j), w_d, acc). */
+ * destination d: D_d(i,j) = upd(D_d(i,j), w_d, acc).  Threads own blocks of MC rows
+ * (the reference's ic loop, my_dgemm.c:168-198) so a packed A block stays in cache. */
+#define MC_PANELS 12 /* 96 rows, DGEMM_MC (common/include/bl_config.h:13) */
 static void chunk_update(int m, int n, int pb, const double *Ap, const double *Bp, int nd, double *const *dst,
                          const double *w, long ldd) {
   const int npi = (m + MR - 1) / MR, npj = (n + NR - 1) / NR;
-#pragma omp parallel for schedule(static)
-  for (int jp = 0; jp < npj; ++jp) {
-    for (int ip = 0; ip < npi; ++ip) {
-      double acc[NR][MR];
-      for (int jj = 0; jj < NR; ++jj)
-        for (int ii = 0; ii < MR; ++ii) acc[jj][ii] = 0.0;
-      const double *a = Ap + (long)ip * pb * MR;
+  const int nblk = (npi + MC_PANELS - 1) / MC_PANELS;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ib = 0; ib < nblk; ++ib) {
+    const int ip0 = ib * MC_PANELS, ip1 = (ip0 + MC_PANELS < npi) ? ip0 + MC_PANELS : npi;
+    for (int jp = 0; jp < npj; ++jp) {
       const double *b = Bp + (long)jp * pb * NR;
-      for (int p = 0; p < pb; ++p) {
+      for (int ip = ip0; ip < ip1; ++ip) {
+        double acc[NR][MR];
+        micro_8x4(pb, Ap + (long)ip * pb * MR, b, acc);
         for (int jj = 0; jj < NR; ++jj) {
-          const double bv = b[p * NR + jj];
-          for (int ii = 0; ii < MR; ++ii) acc[jj][ii] = acc[jj][ii] + a[p * MR + ii] * bv;
-        }
-      }
-      for (int jj = 0; jj < NR; ++jj) {
-        const int j = jp * NR + jj;
-        if (j >= n) break;
-        for (int ii = 0; ii < MR; ++ii) {
-          const int i = ip * MR + ii;
-          if (i >= m) break;
-          for (int d = 0; d < nd; ++d) {
-            double *c = dst[d] + i + (long)j * ldd;
-            *c = upd(*c, w[d], acc[jj][ii]);
+          const int j = jp * NR + jj;
+          if (j >= n) break;
+          for (int ii = 0; ii < MR; ++ii) {
+            const int i = ip * MR + ii;
+            if (i >= m) break;
+            for (int d = 0; d < nd; ++d) {
+              double *c = dst[d] + i + (long)j * ldd;
+              *c = upd(*c, w[d], acc[jj][ii]);
+            }
           }
         }
       }
