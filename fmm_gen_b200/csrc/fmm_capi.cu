@@ -8,6 +8,8 @@
 //   fringe split + peeling         meta/common_mix.py:124-171, common/dgemm/bl_dgemm_util.c:316-353
 //   packing pool                   common/dgemm/bl_dgemm_util.c:375-394 (here: stream-ordered
 //                                  device allocations, freed after each call)
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -211,27 +213,72 @@ fmm_plan* classical_plan() {
 }
 
 bool smem_configured[kMaxDevices];
+int sm_count[kMaxDevices];
+unsigned* dev_status[kMaxDevices];
 std::mutex g_attr_mu;
 
-int configure_kernel() {
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+int configure_kernel(int* dev_out) {
   int dev = 0;
   FMM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
   std::lock_guard<std::mutex> lk(g_attr_mu);
   if (!smem_configured[dev]) {
-    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)fmm::SMEM_BYTES));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::smem_bytes(false)));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::smem_bytes(true)));
+    if (!g_encode_tiled) {
+      cudaDriverEntryPointQueryResult q;
+      void* fn = nullptr;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess)
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    FMM_CUDA_TRY(cudaDeviceGetAttribute(&sm_count[dev], cudaDevAttrMultiProcessorCount, dev));
+    FMM_CUDA_TRY(cudaMalloc(&dev_status[dev], sizeof(unsigned)));
+    FMM_CUDA_TRY(cudaMemset(dev_status[dev], 0, sizeof(unsigned)));
     smem_configured[dev] = true;
   }
+  *dev_out = dev;
   return FMM_OK;
 }
 
-// Launch the DMMA GEMM over sub-blocks of size ms x ks x ns.
-int launch_gemm(int kind, const DevTables& d, int r_begin, int r_end, int mode, const double* A, long long lda,
-                const double* B, long long ldb, double* C, long long ldc, double* M, long long ldm,
+// Column-major FP64 matrix (rows x cols, leading dimension ld) as a 2-D tensor map with
+// the given box.  Returns false when TMA cannot address it (then cp.async staging runs).
+bool make_tensor_map(CUtensorMap* map, const double* base, long long rows, long long cols, long long ld,
+                     unsigned box_rows, unsigned box_cols) {
+  if (!g_encode_tiled) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (ld & 1) != 0) return false;
+  if (rows <= 0 || cols <= 0 || rows >= (1LL << 31) || cols >= (1LL << 31) || ld * 8 >= (1LL << 40)) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(double)};
+  cuuint32_t box[2] = {box_rows, box_cols};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode_tiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Products per tile are split into chunks when there are too few tile positions to fill
+// the persistent grid several times over.
+int choose_chunks(int ntiles, int nprod, int nsm) {
+  const long long want = 16LL * nsm;
+  long long c = (want + ntiles - 1) / ntiles;
+  if (c < 1) c = 1;
+  if (c > nprod) c = nprod;
+  return (int)c;
+}
+
+// Launch the persistent DMMA GEMM over sub-blocks of size ms x ks x ns.
+int launch_gemm(int kind, const DevTables& d, const int grid_dims[3], int nprod, int mode, const double* A,
+                long long lda, const double* B, long long ldb, double* C, long long ldc, double* M, long long ldm,
                 long long m_stride, int ms, int ns, int ks, cudaStream_t st) {
-  if (ms <= 0 || ns <= 0 || ks <= 0 || r_end <= r_begin) return FMM_OK;
-  int rc = configure_kernel();
+  if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
+  int dev = 0;
+  int rc = configure_kernel(&dev);
   if (rc != FMM_OK) return rc;
   fmm::GemmArgs a{};
   a.A = A;
@@ -248,17 +295,43 @@ int launch_gemm(int kind, const DevTables& d, int r_begin, int r_end, int mode, 
   a.ks = ks;
   a.prods = d.prods;
   a.terms = d.terms;
-  a.r_begin = r_begin;
-  a.r_end = r_end;
+  a.nprod = nprod;
   a.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
   a.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
   a.mode = mode;
-  dim3 grid((unsigned)(a.tiles_m * a.tiles_n), mode == fmm::MODE_STORE_M ? (unsigned)(r_end - r_begin) : 1u);
-  ProfScope ps(kind, st);
-  fmm::fmm_gemm_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES, st>>>(a);
+  a.status = dev_status[dev];
+  const int ntiles = a.tiles_m * a.tiles_n;
+  a.chunks = (mode == fmm::MODE_ACCUM_C) ? choose_chunks(ntiles, nprod, sm_count[dev]) : 1;
+  const long long units = (long long)ntiles * (mode == fmm::MODE_STORE_M ? nprod : a.chunks);
+  if (units > INT32_MAX) return FMM_E_UNSUPPORTED;
+  int* tickets = nullptr;
+  if (mode == fmm::MODE_ACCUM_C && a.chunks > 1) {
+    FMM_CUDA_TRY(cudaMallocAsync((void**)&tickets, sizeof(int) * ntiles, st));
+    FMM_CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int) * ntiles, st));
+  }
+  a.tickets = tickets;
+  const unsigned grid = (unsigned)(units < sm_count[dev] ? units : sm_count[dev]);
+  // A spans grid_dims[0] x grid_dims[1] blocks of ms x ks; B grid_dims[1] x grid_dims[2] of ks x ns
+  const bool tma =
+      make_tensor_map(&a.tmA, A, (long long)grid_dims[0] * ms, (long long)grid_dims[1] * ks, lda, fmm::BM, fmm::BK) &&
+      make_tensor_map(&a.tmB, B, (long long)grid_dims[1] * ks, (long long)grid_dims[2] * ns, ldb, fmm::TB_K, fmm::BN);
+  {
+    ProfScope ps(kind, st);
+    if (tma)
+      fmm::fmm_gemm_kernel<true><<<grid, fmm::NTHREADS, fmm::smem_bytes(true), st>>>(a);
+    else
+      fmm::fmm_gemm_kernel<false><<<grid, fmm::NTHREADS, fmm::smem_bytes(false), st>>>(a);
+  }
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  return cuda_status(cudaGetLastError());
+  rc = cuda_status(cudaGetLastError());
+  if (tickets) {
+    cudaError_t fe = cudaFreeAsync(tickets, st);
+    if (rc == FMM_OK) rc = cuda_status(fe);
+  }
+  return rc;
 }
+
+const int kUnitGrid[3] = {1, 1, 1};
 
 int plain_gemm(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, double* C,
                long long ldc, cudaStream_t st) {
@@ -266,7 +339,7 @@ int plain_gemm(int m, int n, int k, const double* A, long long lda, const double
   DevTables* d = nullptr;
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
-  return launch_gemm(K_GEMM_CLASSICAL, *d, 0, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
+  return launch_gemm(K_GEMM_CLASSICAL, *d, kUnitGrid, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
 }
 
 int grid_for(long long total, int threads) {
@@ -322,7 +395,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   const int R = plan->rank;
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
-      rc = launch_gemm(K_GEMM_FMM, *d, 0, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+      rc = launch_gemm(K_GEMM_FMM, *d, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
       if (rc != FMM_OK) return rc;
     } else {
       const long long mstride = (long long)ms * ns;
@@ -336,7 +409,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
       FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes + s_bytes + t_bytes, st));
       double* M = reinterpret_cast<double*>(ws);
       if (pack == FMM_PACK_AB) {
-        rc = launch_gemm(K_GEMM_FMM, *d, 0, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
+        rc = launch_gemm(K_GEMM_FMM, *d, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
       } else {
         double* S = reinterpret_cast<double*>(ws + bytes);
         double* T = reinterpret_cast<double*>(ws + bytes + s_bytes);
@@ -383,7 +456,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
           DevTables* dc = nullptr;
           rc = device_tables(classical_plan(), &dc);
           for (int r = 0; rc == FMM_OK && r < R; ++r) {
-            rc = launch_gemm(K_GEMM_FMM, *dc, 0, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
+            rc = launch_gemm(K_GEMM_FMM, *dc, kUnitGrid, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
                              T + (long long)r * ks * ns, ks, nullptr, 0, M + (long long)r * mstride, ms, 0, ms, ns,
                              ks, st);
           }
@@ -415,6 +488,17 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
     }
   }
   return peel(m, n, k, A, lda, B, ldb, C, ldc, pm, pk, pn, st);
+}
+
+int device_status(bool clear) {
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
+  if (!smem_configured[dev]) return FMM_OK;
+  unsigned v = 0;
+  FMM_CUDA_TRY(cudaMemcpy(&v, dev_status[dev], sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (clear && v) FMM_CUDA_TRY(cudaMemset(dev_status[dev], 0, sizeof(unsigned)));
+  return v ? FMM_E_TIMEOUT : FMM_OK;
 }
 
 // Host-pointer execution: stage A, B, C into device memory, run, copy C back.
@@ -449,6 +533,7 @@ int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, co
   cudaFreeAsync(dC, st);
   cudaError_t se = cudaStreamSynchronize(st);
   if (rc == FMM_OK) rc = cuda_status(se);
+  if (rc == FMM_OK) rc = device_status(true);
   return rc;
 }
 
@@ -561,6 +646,7 @@ void bl_dynamic_peeling(int m, int n, int k, double* A, int lda, double* B, int 
   if (dC) cudaFreeAsync(dC, st);
   cudaError_t se = cudaStreamSynchronize(st);
   if (rc == FMM_OK) rc = cuda_status(se);
+  if (rc == FMM_OK) rc = device_status(true);
   t_last_error = rc;
 }
 
@@ -581,6 +667,8 @@ const char* fmm_error_string(int code) {
 }
 
 long long fmm_kernel_launch_count(void) { return g_launches.load(); }
+
+int fmm_device_status(int clear) { return device_status(clear != 0); }
 
 int fmm_profile_begin(void) {
   std::lock_guard<std::mutex> lk(g_prof_mu);

@@ -1,39 +1,74 @@
-// fmm_b200 device code: FP64 DMMA GEMM mainloop with fused operand linear combinations
-// and a multi-destination epilogue, plus the elementwise helpers of the AB / NAIVE
+// fmm_b200 device code: a persistent, warp-specialised FP64 DMMA GEMM whose producer
+// warpgroup forms the U/V linear combinations of A and B sub-blocks while staging them
+// into shared memory, and whose consumer warpgroups scatter each product into every C
+// block with a nonzero W coefficient; plus the elementwise kernels of the AB / NAIVE
 // pack types.  sm_100a only.
 //
 // Mapping of the reference's CPU design (fmm-gen):
 //   * BLIS packing with fused sums (meta/abc_gen_mix.py:171-251, packA/B_add_stra_abc<r>)
-//     -> cp.async staging of every U/V term tile into thread-private shared-memory
-//        slots, summed once per CTA tile into the operand buffer.
+//     -> producer warpgroup: cp.async of every U/V term tile into thread-private
+//        shared-memory slots, folded into the operand stage (sum with coefficients),
+//        released to the consumers with an mbarrier.
 //   * AVX 8x4 micro-kernel (common/kernels/bl_dgemm_asm_8x4.c)
-//     -> 128x128x16 CTA tile of mma.sync.m16n8k4 FP64 (DMMA) fragments.
+//     -> 128x128 CTA tile of mma.sync.m16n8k4 FP64 (DMMA) fragments, 8 consumer warps
+//        with 64x32 warp tiles.
 //   * multi-destination C update (meta/abc_micro_kernel_gen.py:147-244)
-//     -> epilogue C_l += W[l,r] * M_r for every nonzero W of product r, done by the
-//        CTA that owns the tile position in all C blocks, so no two CTAs ever touch
-//        the same C element (no atomics, deterministic).
+//     -> epilogue C_l += W[l,r] * M_r for every nonzero W of product r.  A work unit
+//        owns one tile position in all C blocks for a range of products; when products
+//        are split over several units, per-tile tickets order the units' C updates
+//        (bounded spin, error flag on timeout), so no two CTAs ever update the same C
+//        element at once and products are applied in order r = 0..R-1.
 //   * M_Add / S_Add / T_Add (meta/ab_gen_mix.py:341-372, meta/naive_gen_mix.py:60-137)
 //     -> fmm_scatter_kernel / fmm_lincomb_kernel.
 #pragma once
-#include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 namespace fmm {
 
 constexpr int BM = 128;   // CTA tile rows (m)
 constexpr int BN = 128;   // CTA tile columns (n)
-constexpr int BK = 16;    // k depth of one staged tile
-constexpr int NTHREADS = 256;
+constexpr int BK = 8;     // k depth of one operand stage
+constexpr int NPROD = 128;               // producer threads (warpgroup 0)
+constexpr int NCONS = 256;               // consumer threads (warpgroups 1, 2)
+constexpr int NTHREADS = NPROD + NCONS;  // 384
 constexpr int LDA_S = BM + 4;  // opA[k][m], padded: conflict-free fragment loads
 constexpr int LDB_S = BK + 4;  // opB[n][k]
-constexpr int NRAW = 4;        // thread-private raw term slots in flight
-constexpr int EA = BM * BK / NTHREADS;  // A elements a thread stages per term (8)
-constexpr int EB = BN * BK / NTHREADS;  // B elements a thread stages per term (8)
+constexpr int NSTAGE = 4;      // operand stages (producer -> consumers)
+constexpr int NRAW = 8;        // thread-private raw term slots in flight per producer thread
+constexpr int EA = BM * BK / NPROD;  // A elements a producer thread stages per term (8)
+constexpr int EB = BN * BK / NPROD;  // B elements a producer thread stages per term (8)
 constexpr int OPA_SZ = BK * LDA_S;
 constexpr int OPB_SZ = BN * LDB_S;
-constexpr int RAW_SZ = (EA + EB) * NTHREADS;
-constexpr size_t SMEM_BYTES = (size_t)(2 * OPA_SZ + 2 * OPB_SZ + NRAW * RAW_SZ) * sizeof(double);
-constexpr int GROUP_M = 8;     // tile raster: groups of 8 tile rows for L2 reuse
+constexpr int STAGE_SZ = OPA_SZ + OPB_SZ;
+constexpr int RAW_SZ = (EA + EB) * NPROD;
+// TMA staging: one raw slot holds an A term box (BK x BM, m contiguous) and a B term box
+// (BN columns of BK + 2 k values, k contiguous; two wider so that a box can start at the
+// even k coordinate at or below an odd one).
+constexpr int TB_K = BK + 2;
+constexpr int TRAW_A = BK * BM;
+constexpr int TRAW_SZ = TRAW_A + BN * TB_K;
+constexpr int NRAW_TMA = 7;
+constexpr unsigned TMA_BYTES_A = TRAW_A * sizeof(double);
+constexpr unsigned TMA_BYTES_B = BN * TB_K * sizeof(double);
+static_assert((NSTAGE * STAGE_SZ * sizeof(double)) % 128 == 0, "raw slots must start 128-byte aligned");
+static_assert((TRAW_SZ * sizeof(double)) % 128 == 0, "TMA raw slots must be 128-byte aligned");
+static_assert((TRAW_A * sizeof(double)) % 128 == 0, "TMA B box must be 128-byte aligned");
+constexpr size_t SMEM_BYTES_CPASYNC =
+    (size_t)(NSTAGE * STAGE_SZ + NRAW * RAW_SZ) * sizeof(double) + 2 * NSTAGE * sizeof(unsigned long long);
+constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_SZ) * sizeof(double) +
+                                  (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long);
+constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
+constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
+constexpr int PROD_REGS = 72;
+constexpr int CONS_REGS = 216;
+static_assert(4 * 32 * PROD_REGS + 8 * 32 * CONS_REGS <= NTHREADS * 168, "register split exceeds the launch budget");
+constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ULL;  // bounded device-side waits give up after 4 s
+// try_wait suspends the waiting thread until the phase completes or this many ns pass,
+// so waiting warps do not take issue slots from the warps they wait for.
+constexpr unsigned MBAR_SUSPEND_NS = 20000;
 
 struct Term {
   int row;      // global block row in the composed grid
@@ -49,7 +84,11 @@ struct Prod {
 
 enum Mode : int { MODE_ACCUM_C = 0, MODE_STORE_M = 1 };
 
+enum StatusBits : unsigned { STATUS_TICKET_TIMEOUT = 1u, STATUS_WAIT_TIMEOUT = 2u };
+
 struct GemmArgs {
+  CUtensorMap tmA;  // whole-matrix tensor maps (TMA path): A (m x k), B (k x n), FP64
+  CUtensorMap tmB;
   const double* A;
   long long lda;
   const double* B;
@@ -62,9 +101,12 @@ struct GemmArgs {
   int ms, ns, ks;   // sub-block sizes
   const Prod* prods;
   const Term* terms;
-  int r_begin, r_end;   // products handled (MODE_ACCUM_C: every CTA loops over all of them)
+  int nprod;        // products [0, nprod)
   int tiles_m, tiles_n;
+  int chunks;       // products are split into `chunks` consecutive ranges per tile
   int mode;
+  int* tickets;     // per tile: chunks completed (zeroed before launch); used when chunks > 1
+  unsigned* status; // device status word (StatusBits)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -74,10 +116,85 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) {
 __device__ __forceinline__ void cp_async8(unsigned dst, const void* src, int src_bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
+__device__ __forceinline__ void cp_async16(unsigned dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile(
+      "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(bar),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+  asm volatile(
+      "{\n .reg .b64 st;\n mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n}\n" ::"r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(MBAR_SUSPEND_NS)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase with the given parity.  Every phase is completed by the
+// other warpgroup of the same CTA, so in a correct run the wait ends; if it has not
+// after WAIT_LIMIT_NS, the status word gets STATUS_WAIT_TIMEOUT and every later wait
+// of every CTA returns at once, so the kernel still finishes and the host reports
+// FMM_E_TIMEOUT.
+__device__ __forceinline__ void mbar_wait(unsigned bar, unsigned parity, unsigned* status) {
+  if (mbar_try_wait(bar, parity)) return;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*(volatile unsigned*)status != 0u) return;
+    if (global_ns() - t0 > WAIT_LIMIT_NS) {
+      atomicOr(status, STATUS_WAIT_TIMEOUT);
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2], double b) {
@@ -87,76 +204,350 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2]
       : "d"(a[0]), "d"(a[1]), "d"(b));
 }
 
-// Position of one load unit = (product, k step, term) in the flattened stream.
-struct UnitIter {
-  int r, s, t;
-  int T;        // max(na, nb) of product r
-};
-
 __device__ __forceinline__ int prod_T(const Prod& p) { return p.na > p.nb ? p.na : p.nb; }
 
-// Issue the cp.async copies of one unit: term t of product r at k step s.
-__device__ __forceinline__ void issue_unit(const GemmArgs& a, const Prod& p, int s, int t, double* raw_slot,
-                                           int m0, int n0, int tid) {
+// Work unit u -> (tile position, product range).  Chunk-major order, so the units of
+// one tile are gridDim.x-strided apart and a later chunk starts well after the earlier.
+struct Unit {
+  int m0, n0, tile, r0, r1;
+};
+
+__device__ __forceinline__ Unit decode_unit(const GemmArgs& a, int u) {
+  const int ntiles = a.tiles_m * a.tiles_n;
+  Unit w;
+  int c, bid;
+  if (a.mode == MODE_STORE_M) {
+    c = u / ntiles;  // one product per unit
+    bid = u % ntiles;
+    w.r0 = c;
+    w.r1 = c + 1;
+  } else {
+    c = u / ntiles;
+    bid = u % ntiles;
+    w.r0 = (int)((long long)a.nprod * c / a.chunks);
+    w.r1 = (int)((long long)a.nprod * (c + 1) / a.chunks);
+  }
+  const int per_group = GROUP_M * a.tiles_n;
+  const int grp = bid / per_group;
+  const int first_m = grp * GROUP_M;
+  const int rows_here = min(a.tiles_m - first_m, GROUP_M);
+  const int in_grp = bid % per_group;
+  const int tile_m = first_m + in_grp % rows_here;
+  const int tile_n = in_grp / rows_here;
+  w.m0 = tile_m * BM;
+  w.n0 = tile_n * BN;
+  w.tile = bid;
+  return w;
+}
+
+__device__ __forceinline__ int num_units(const GemmArgs& a) {
+  const int ntiles = a.tiles_m * a.tiles_n;
+  return ntiles * (a.mode == MODE_STORE_M ? a.nprod : a.chunks);
+}
+
+// ------------------------------------------------------------------------------------
+// Producer: flattened stream of load units (k step s, term t) over the CTA's work units.
+// ------------------------------------------------------------------------------------
+struct LoadIter {
+  int u;            // work unit index (global)
+  Unit w;
+  int r;            // product
+  Prod p;
+  int T;
+  int s, t;
+  bool valid;
+  // term t of product r, fetched when the iterator moves so that the global loads are
+  // off the producer's critical path
+  Term ta, tb;
+};
+
+__device__ __forceinline__ void load_terms(const GemmArgs& a, LoadIter& it) {
+  if (it.t < it.p.na) it.ta = a.terms[it.p.a0 + it.t];
+  if (it.t < it.p.nb) it.tb = a.terms[it.p.b0 + it.t];
+}
+
+__device__ __forceinline__ void load_iter_start(const GemmArgs& a, LoadIter& it, int nks) {
+  it.u = blockIdx.x;
+  it.valid = it.u < num_units(a) && nks > 0;
+  if (!it.valid) return;
+  it.w = decode_unit(a, it.u);
+  it.r = it.w.r0;
+  it.p = a.prods[it.r];
+  it.T = prod_T(it.p);
+  it.s = 0;
+  it.t = 0;
+  load_terms(a, it);
+}
+
+__device__ __forceinline__ void load_iter_next(const GemmArgs& a, LoadIter& it, int nks) {
+  if (++it.t < it.T) {
+    load_terms(a, it);
+    return;
+  }
+  it.t = 0;
+  if (++it.s < nks) {
+    if (it.T > 1) load_terms(a, it);
+    return;
+  }
+  it.s = 0;
+  if (++it.r < it.w.r1) {
+    it.p = a.prods[it.r];
+    it.T = prod_T(it.p);
+    load_terms(a, it);
+    return;
+  }
+  it.u += gridDim.x;
+  if (it.u >= num_units(a)) {
+    it.valid = false;
+    return;
+  }
+  it.w = decode_unit(a, it.u);
+  it.r = it.w.r0;
+  it.p = a.prods[it.r];
+  it.T = prod_T(it.p);
+  load_terms(a, it);
+}
+
+// Raw slot layout (thread-private, conflict-free): pair e of A at [e][pt] (16 B each),
+// then the B pairs.  A term tile: 128 (m) x 8 (k) = 512 m-pairs, 4 per thread; B term
+// tile: 8 (k) x 128 (n) = 512 k-pairs, 4 per thread.
+constexpr int PA = EA / 2;  // A pairs per thread per term
+constexpr int PB = EB / 2;
+
+__device__ __forceinline__ void issue_unit(const GemmArgs& a, const LoadIter& it, double* raw_slot, int pt) {
   const unsigned sbase = smem_u32(raw_slot);
-  if (t < p.na) {
-    const Term tm = a.terms[p.a0 + t];
-    const double* base = a.A + (long long)tm.row * a.ms + (long long)tm.col * a.ks * a.lda;
+  if (it.t < it.p.na) {
+    const long long off = (long long)it.ta.row * a.ms + (long long)it.ta.col * a.ks * a.lda;
+    const double* base = a.A + off;
+    const bool al16 = ((off & 1) == 0) && ((a.lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(a.A) & 15) == 0);
 #pragma unroll
-    for (int e = 0; e < EA; ++e) {
-      const int idx = e * NTHREADS + tid;
-      const int mm = idx % BM, kk = idx / BM;
-      const int gm = m0 + mm, gk = s * BK + kk;
-      const bool v = (gm < a.ms) && (gk < a.ks);
-      const double* src = v ? base + gm + (long long)gk * a.lda : a.A;
-      cp_async8(sbase + (unsigned)(idx * sizeof(double)), src, v ? 8 : 0);
+    for (int e = 0; e < PA; ++e) {
+      const int q = e * NPROD + pt;        // pair index
+      const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+      const int gm = it.w.m0 + mm, gk = it.s * BK + kk;
+      const unsigned dst = sbase + (unsigned)(q * 16);
+      if (al16) {
+        const int nb = (gk < a.ks) ? ((gm + 1 < a.ms) ? 16 : (gm < a.ms ? 8 : 0)) : 0;
+        cp_async16(dst, nb ? base + gm + (long long)gk * a.lda : a.A, nb);
+      } else {
+        const bool v0 = (gk < a.ks) && (gm < a.ms), v1 = (gk < a.ks) && (gm + 1 < a.ms);
+        cp_async8(dst, v0 ? base + gm + (long long)gk * a.lda : a.A, v0 ? 8 : 0);
+        cp_async8(dst + 8, v1 ? base + gm + 1 + (long long)gk * a.lda : a.A, v1 ? 8 : 0);
+      }
     }
   }
-  if (t < p.nb) {
-    const Term tm = a.terms[p.b0 + t];
-    const double* base = a.B + (long long)tm.row * a.ks + (long long)tm.col * a.ns * a.ldb;
+  if (it.t < it.p.nb) {
+    const long long off = (long long)it.tb.row * a.ks + (long long)it.tb.col * a.ns * a.ldb;
+    const double* base = a.B + off;
+    const bool al16 = ((off & 1) == 0) && ((a.ldb & 1) == 0) && ((reinterpret_cast<uintptr_t>(a.B) & 15) == 0);
 #pragma unroll
-    for (int e = 0; e < EB; ++e) {
-      const int idx = e * NTHREADS + tid;
-      const int kk = idx % BK, nn = idx / BK;
-      const int gk = s * BK + kk, gn = n0 + nn;
-      const bool v = (gk < a.ks) && (gn < a.ns);
-      const double* src = v ? base + gk + (long long)gn * a.ldb : a.B;
-      cp_async8(sbase + (unsigned)((EA * NTHREADS + idx) * sizeof(double)), src, v ? 8 : 0);
-    }
-  }
-}
-
-// Fold one staged term into the operand buffers.  A thread reads back only the
-// elements it copied itself, so no barrier is needed between arrival and use.
-__device__ __forceinline__ void consume_unit(const GemmArgs& a, const Prod& p, int t, const double* raw_slot,
-                                             double* opA, double* opB, int tid) {
-  if (t < p.na) {
-    const double c = a.terms[p.a0 + t].coef;
-#pragma unroll
-    for (int e = 0; e < EA; ++e) {
-      const int idx = e * NTHREADS + tid;
-      const int mm = idx % BM, kk = idx / BM;
-      const double v = raw_slot[idx];
-      double* dst = opA + kk * LDA_S + mm;
-      *dst = (t == 0) ? c * v : fma(c, v, *dst);
-    }
-  }
-  if (t < p.nb) {
-    const double c = a.terms[p.b0 + t].coef;
-#pragma unroll
-    for (int e = 0; e < EB; ++e) {
-      const int idx = e * NTHREADS + tid;
-      const int kk = idx % BK, nn = idx / BK;
-      const double v = raw_slot[EA * NTHREADS + idx];
-      double* dst = opB + nn * LDB_S + kk;
-      *dst = (t == 0) ? c * v : fma(c, v, *dst);
+    for (int e = 0; e < PB; ++e) {
+      const int q = e * NPROD + pt;
+      const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
+      const int gk = it.s * BK + kk, gn = it.w.n0 + nn;
+      const unsigned dst = sbase + (unsigned)((PA * NPROD + q) * 16);
+      if (al16) {
+        const int nb = (gn < a.ns) ? ((gk + 1 < a.ks) ? 16 : (gk < a.ks ? 8 : 0)) : 0;
+        cp_async16(dst, nb ? base + gk + (long long)gn * a.ldb : a.B, nb);
+      } else {
+        const bool v0 = (gn < a.ns) && (gk < a.ks), v1 = (gn < a.ns) && (gk + 1 < a.ks);
+        cp_async8(dst, v0 ? base + gk + (long long)gn * a.ldb : a.B, v0 ? 8 : 0);
+        cp_async8(dst + 8, v1 ? base + gk + 1 + (long long)gn * a.ldb : a.B, v1 ? 8 : 0);
+      }
     }
   }
 }
 
-__device__ __forceinline__ void mma_tile(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
-                                         int wn, int g, int t4) {
+// Fold one staged term into the operand stage.  A producer thread reads back only the
+// elements it copied itself, so no barrier is needed between arrival and use; the
+// stage itself belongs to the producer between its empty and full barrier phases.
+__device__ __forceinline__ void fold_unit(const LoadIter& it, const double* raw_slot, double* opA, double* opB,
+                                          int pt) {
+  if (it.t < it.p.na) {
+    const double c = it.ta.coef;
+#pragma unroll
+    for (int e = 0; e < PA; ++e) {
+      const int q = e * NPROD + pt;
+      const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+      const double2 v = reinterpret_cast<const double2*>(raw_slot)[q];
+      double2* dst = reinterpret_cast<double2*>(opA + kk * LDA_S + mm);
+      if (it.t == 0) {
+        *dst = make_double2(c * v.x, c * v.y);
+      } else {
+        const double2 o = *dst;
+        *dst = make_double2(fma(c, v.x, o.x), fma(c, v.y, o.y));
+      }
+    }
+  }
+  if (it.t < it.p.nb) {
+    const double c = it.tb.coef;
+#pragma unroll
+    for (int e = 0; e < PB; ++e) {
+      const int q = e * NPROD + pt;
+      const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
+      const double2 v = reinterpret_cast<const double2*>(raw_slot)[PA * NPROD + q];
+      double2* dst = reinterpret_cast<double2*>(opB + nn * LDB_S + kk);
+      if (it.t == 0) {
+        *dst = make_double2(c * v.x, c * v.y);
+      } else {
+        const double2 o = *dst;
+        *dst = make_double2(fma(c, v.x, o.x), fma(c, v.y, o.y));
+      }
+    }
+  }
+}
+
+__device__ void producer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0, int pt,
+                         int nks) {
+  LoadIter iss, con;
+  load_iter_start(a, iss, nks);
+  load_iter_start(a, con, nks);
+  // prologue: NRAW - 1 load units in flight
+#pragma unroll 1
+  for (int i = 0; i < NRAW - 1; ++i) {
+    if (iss.valid) {
+      issue_unit(a, iss, raw + (size_t)(i % NRAW) * RAW_SZ, pt);
+      load_iter_next(a, iss, nks);
+    }
+    cp_async_commit();
+  }
+  long long kc = 0;  // operand stages filled so far
+  int unit = 0;
+#pragma unroll 1
+  while (con.valid) {
+    const int stage = (int)(kc % NSTAGE);
+    double* opA = stages + (size_t)stage * STAGE_SZ;
+    double* opB = opA + OPA_SZ;
+    if (con.t == 0) mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    cp_async_wait<NRAW - 2>();
+    fold_unit(con, raw + (size_t)(unit % NRAW) * RAW_SZ, opA, opB, pt);
+    const bool last_term = (con.t == con.T - 1);
+    if (iss.valid) {
+      issue_unit(a, iss, raw + (size_t)((unit + NRAW - 1) % NRAW) * RAW_SZ, pt);
+      load_iter_next(a, iss, nks);
+    }
+    cp_async_commit();
+    ++unit;
+    if (last_term) {
+      __syncwarp();
+      if ((pt & 31) == 0) mbar_arrive(full0 + 8 * stage);
+      ++kc;
+    }
+    load_iter_next(a, con, nks);
+  }
+  cp_async_wait<0>();
+}
+
+// ------------------------------------------------------------------------------------
+// TMA producer: thread 0 issues one or two tensor copies per load unit into a raw slot
+// (completion counted in bytes on raw_full[slot]); all 128 producer threads then fold
+// the slot into the operand stage and release it on raw_empty[slot].
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void issue_unit_tma(const GemmArgs& a, const LoadIter& it, double* raw_slot,
+                                               unsigned bar) {
+  const bool hasA = it.t < it.p.na, hasB = it.t < it.p.nb;
+  mbar_arrive_expect_tx(bar, (hasA ? TMA_BYTES_A : 0u) + (hasB ? TMA_BYTES_B : 0u));
+  const int k0 = it.s * BK;
+  if (hasA) {
+    // x = m coordinate: row * ms + m0 is even (ms is a multiple of 8, m0 of 128)
+    tma_load_2d(smem_u32(raw_slot), &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, bar);
+  }
+  if (hasB) {
+    const int xk = it.tb.row * a.ks + k0;  // k coordinate; rounded down to even
+    tma_load_2d(smem_u32(raw_slot + TRAW_A), &a.tmB, xk & ~1, it.tb.col * a.ns + it.w.n0, bar);
+  }
+}
+
+__device__ __forceinline__ void fold_unit_tma(const GemmArgs& a, const LoadIter& it, const double* raw_slot,
+                                              double* opA, double* opB, int pt) {
+  const int k0 = it.s * BK;
+  if (it.t < it.p.na) {
+    const double c = it.ta.coef;
+#pragma unroll
+    for (int e = 0; e < PA; ++e) {
+      const int q = e * NPROD + pt;
+      const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+      double2 v = reinterpret_cast<const double2*>(raw_slot)[(kk * BM + mm) / 2];
+      if (k0 + kk >= a.ks) v = make_double2(0.0, 0.0);  // past the sub-block's k range
+      double2* dst = reinterpret_cast<double2*>(opA + kk * LDA_S + mm);
+      if (it.t == 0) {
+        *dst = make_double2(c * v.x, c * v.y);
+      } else {
+        const double2 o = *dst;
+        *dst = make_double2(fma(c, v.x, o.x), fma(c, v.y, o.y));
+      }
+    }
+  }
+  if (it.t < it.p.nb) {
+    const double c = it.tb.coef;
+    const int shift = (it.tb.row * a.ks) & 1;
+    const double* rb = raw_slot + TRAW_A;
+#pragma unroll
+    for (int e = 0; e < PB; ++e) {
+      const int q = e * NPROD + pt;
+      const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
+      double v0 = rb[nn * TB_K + kk + shift], v1 = rb[nn * TB_K + kk + 1 + shift];
+      if (k0 + kk >= a.ks) v0 = 0.0;
+      if (k0 + kk + 1 >= a.ks) v1 = 0.0;
+      double2* dst = reinterpret_cast<double2*>(opB + nn * LDB_S + kk);
+      if (it.t == 0) {
+        *dst = make_double2(c * v0, c * v1);
+      } else {
+        const double2 o = *dst;
+        *dst = make_double2(fma(c, v0, o.x), fma(c, v1, o.y));
+      }
+    }
+  }
+}
+
+__device__ void producer_tma(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0,
+                             unsigned rfull0, unsigned rempty0, int pt, int nks) {
+  LoadIter iss, con;
+  load_iter_start(a, iss, nks);
+  load_iter_start(a, con, nks);
+  if (pt == 0) {
+#pragma unroll 1
+    for (int i = 0; i < NRAW_TMA - 1 && iss.valid; ++i) {
+      issue_unit_tma(a, iss, raw + (size_t)i * TRAW_SZ, rfull0 + 8 * i);
+      load_iter_next(a, iss, nks);
+    }
+  }
+  long long kc = 0;
+  long long unit = 0;
+#pragma unroll 1
+  while (con.valid) {
+    const int stage = (int)(kc % NSTAGE);
+    double* opA = stages + (size_t)stage * STAGE_SZ;
+    double* opB = opA + OPA_SZ;
+    if (con.t == 0) mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    const int slot = (int)(unit % NRAW_TMA);
+    mbar_wait(rfull0 + 8 * slot, (unsigned)((unit / NRAW_TMA) & 1), a.status);
+    fold_unit_tma(a, con, raw + (size_t)slot * TRAW_SZ, opA, opB, pt);
+    __syncwarp();
+    if ((pt & 31) == 0) mbar_arrive(rempty0 + 8 * slot);
+    if (con.t == con.T - 1) {
+      if ((pt & 31) == 0) mbar_arrive(full0 + 8 * stage);
+      ++kc;
+    }
+    if (pt == 0 && iss.valid) {
+      // unit + NRAW_TMA - 1 reuses the slot of unit - 1: wait until every producer warp
+      // has folded it
+      const long long nu = unit + NRAW_TMA - 1;
+      const int islot = (int)(nu % NRAW_TMA);
+      if (unit >= 1) mbar_wait(rempty0 + 8 * islot, (unsigned)(((unit - 1) / NRAW_TMA) & 1), a.status);
+      issue_unit_tma(a, iss, raw + (size_t)islot * TRAW_SZ, rfull0 + 8 * islot);
+      load_iter_next(a, iss, nks);
+    }
+    ++unit;
+    load_iter_next(a, con, nks);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Consumers: DMMA over the stages, then the multi-destination epilogue.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void mma_stage(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
+                                          int wn, int g, int t4) {
 #pragma unroll
   for (int kq = 0; kq < BK / 4; ++kq) {
     double af[4][2], bf[4];
@@ -196,6 +587,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
           }
     return;
   }
+#pragma unroll 1
   for (int c = 0; c < p.nc; ++c) {
     const Term tm = a.terms[p.c0 + c];
     const double w = tm.coef;
@@ -218,102 +610,111 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
   }
 }
 
-// One CTA computes one BMxBN tile position for products [r_begin, r_end) in order
-// (MODE_ACCUM_C), or for the single product blockIdx.y + r_begin (MODE_STORE_M).
-__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const GemmArgs a) {
-  extern __shared__ __align__(16) double smem[];
-  double* opA = smem;                    // [2][OPA_SZ]
-  double* opB = smem + 2 * OPA_SZ;       // [2][OPB_SZ]
-  double* raw = opB + 2 * OPB_SZ;        // [NRAW][RAW_SZ]
+// Wait until the previous product chunk of this tile has finished its C updates.
+__device__ __forceinline__ void ticket_wait(const GemmArgs& a, int tile, int chunk, int ct) {
+  if (ct == 0) {
+    const int* tp = a.tickets + tile;
+    if (ld_acquire(tp) < chunk) {
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire(tp) < chunk) {
+        if (*(volatile unsigned*)a.status != 0u) break;
+        if (global_ns() - t0 > WAIT_LIMIT_NS) {
+          atomicOr(a.status, STATUS_TICKET_TIMEOUT);
+          break;
+        }
+        __nanosleep(256);
+      }
+    }
+  }
+  named_bar_sync(1, NCONS);
+}
 
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
+__device__ __forceinline__ void ticket_release(const GemmArgs& a, int tile, int chunk, int ct) {
+  __threadfence();
+  named_bar_sync(1, NCONS);
+  if (ct == 0) st_release(a.tickets + tile, chunk + 1);
+}
+
+__device__ void consumer(const GemmArgs& a, const double* stages, unsigned full0, unsigned empty0, int ct, int nks) {
+  const int warp = ct >> 5, lane = ct & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
-
-  // Grouped raster over tile positions.
-  const int bid = blockIdx.x;
-  const int group_rows = GROUP_M;
-  const int per_group = group_rows * a.tiles_n;
-  const int grp = bid / per_group;
-  const int first_m = grp * group_rows;
-  const int rows_here = min(a.tiles_m - first_m, group_rows);
-  const int in_grp = bid % per_group;
-  const int tile_m = first_m + in_grp % rows_here;
-  const int tile_n = in_grp / rows_here;
-  const int m0 = tile_m * BM, n0 = tile_n * BN;
-
-  int rb = a.r_begin, re = a.r_end;
-  if (a.mode == MODE_STORE_M) {
-    rb = a.r_begin + blockIdx.y;
-    re = rb + 1;
-  }
-  const int nks = (a.ks + BK - 1) / BK;
-
-  // Issue iterator.
-  int ir = rb, is = 0, it = 0;
-  Prod ip = a.prods[ir];
-  int iT = prod_T(ip);
-  bool issuing = true;
-  auto advance_issue = [&]() {
-    if (++it < iT) return;
-    it = 0;
-    if (++is < nks) return;
-    is = 0;
-    if (++ir < re) {
-      ip = a.prods[ir];
-      iT = prod_T(ip);
-    } else {
-      issuing = false;
-    }
-  };
-
-  int unit = 0;
-#pragma unroll 1
-  for (int i = 0; i < NRAW - 1; ++i) {
-    if (issuing) {
-      issue_unit(a, ip, is, it, raw + (size_t)((unit + i) % NRAW) * RAW_SZ, m0, n0, tid);
-      advance_issue();
-    }
-    cp_async_commit();
-  }
-
-  int kcount = 0;
+  const int nunits = num_units(a);
+  const int ntiles = a.tiles_m * a.tiles_n;
+  const bool ordered = (a.mode == MODE_ACCUM_C) && a.chunks > 1;
+  long long kc = 0;
   double acc[4][4][4];
 #pragma unroll 1
-  for (int r = rb; r < re; ++r) {
-    const Prod p = a.prods[r];
-    const int T = prod_T(p);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
-
+  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const Unit w = decode_unit(a, u);
+    const int chunk = u / ntiles;
 #pragma unroll 1
-    for (int s = 0; s < nks; ++s) {
-      const int buf = kcount & 1;
-      double* oa = opA + buf * OPA_SZ;
-      double* ob = opB + buf * OPB_SZ;
+    for (int r = w.r0; r < w.r1; ++r) {
+      const Prod p = a.prods[r];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 #pragma unroll 1
-      for (int t = 0; t < T; ++t) {
-        cp_async_wait<NRAW - 2>();
-        consume_unit(a, p, t, raw + (size_t)(unit % NRAW) * RAW_SZ, oa, ob, tid);
-        if (issuing) {
-          issue_unit(a, ip, is, it, raw + (size_t)((unit + NRAW - 1) % NRAW) * RAW_SZ, m0, n0, tid);
-          advance_issue();
-        }
-        cp_async_commit();
-        ++unit;
+      for (int s = 0; s < nks; ++s) {
+        const int stage = (int)(kc % NSTAGE);
+        const double* opA = stages + (size_t)stage * STAGE_SZ;
+        const double* opB = opA + OPA_SZ;
+        mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), a.status);
+        mma_stage(opA, opB, acc, wm, wn, g, t4);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * stage);
+        ++kc;
       }
-      __syncthreads();
-      mma_tile(oa, ob, acc, wm, wn, g, t4);
-      ++kcount;
+      if (ordered && r == w.r0) ticket_wait(a, w.tile, chunk, ct);
+      epilogue(a, p, r, acc, w.m0, w.n0, wm, wn, g, t4);
     }
-    epilogue(a, p, r, acc, m0, n0, wm, wn, g, t4);
+    if (ordered) ticket_release(a, w.tile, chunk, ct);
   }
-  cp_async_wait<0>();
+}
+
+// Persistent: one CTA per SM walks work units blockIdx.x, blockIdx.x + gridDim.x, ...
+// TMA = true stages operands with tensor copies (A, B 16-byte aligned, even leading
+// dimensions); TMA = false with per-thread cp.async (any alignment).
+template <bool TMA>
+__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_constant__ GemmArgs a) {
+  extern __shared__ __align__(128) double smem[];
+  double* stages = smem;                                  // [NSTAGE][STAGE_SZ]
+  double* raw = stages + (size_t)NSTAGE * STAGE_SZ;       // [NRAW][RAW_SZ] or [NRAW_TMA][TRAW_SZ]
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(raw + (TMA ? (size_t)NRAW_TMA * TRAW_SZ : (size_t)NRAW * RAW_SZ));
+  const unsigned full0 = smem_u32(bars);
+  const unsigned empty0 = smem_u32(bars + NSTAGE);
+  const unsigned rfull0 = smem_u32(bars + 2 * NSTAGE);
+  const unsigned rempty0 = smem_u32(bars + 2 * NSTAGE + NRAW_TMA);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(full0 + 8 * s, NPROD / 32);
+      mbar_init(empty0 + 8 * s, NCONS / 32);
+    }
+    if (TMA) {
+      for (int s = 0; s < NRAW_TMA; ++s) {
+        mbar_init(rfull0 + 8 * s, 1);
+        mbar_init(rempty0 + 8 * s, NPROD / 32);
+      }
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const int nks = (a.ks + BK - 1) / BK;
+  if (tid < NPROD) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
+    if (TMA)
+      producer_tma(a, stages, raw, full0, empty0, rfull0, rempty0, tid, nks);
+    else
+      producer(a, stages, raw, full0, empty0, tid, nks);
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
+    consumer(a, stages, full0, empty0, tid - NPROD, nks);
+  }
 }
 
 // S_r / T_r temporaries of the NAIVE pack type: out_r = sum_t coef_t * X_{blk_t}.

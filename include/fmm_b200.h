@@ -95,6 +95,12 @@ int fmm_plain_dgemm_dev(int m, int n, int k, const double *A, long lda, const do
 int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, const double *A, int lda,
                    const double *B, int ldb, double *C, int ldc);
 
+/* Device-side status of the current device: FMM_E_TIMEOUT if a bounded wait inside a
+ * kernel gave up since the last clear (results of that call are then unreliable),
+ * FMM_OK otherwise.  Synchronises with the device; clear != 0 resets the word.  The
+ * synchronous host entry points check it themselves. */
+int fmm_device_status(int clear);
+
 /* Number of kernels the library launched since load (all entry points, all streams). */
 long long fmm_kernel_launch_count(void);
 
