@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -171,6 +172,17 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
         p->terms.push_back(fmm::Term{rows[pos], cols[pos], coefs[pos]});
       }
     }
+    // A single operand term whose coefficient is a power of two moves its coefficient
+    // into the product's W coefficients (exact), so the operand can be staged as is.
+    for (int side = 0; side < 2; ++side) {
+      const int n = side == 0 ? pr.na : pr.nb;
+      fmm::Term& t = p->terms[side == 0 ? pr.a0 : pr.b0];
+      int e2 = 0;
+      if (n == 1 && t.coef != 1.0 && t.coef != 0.0 && std::frexp(std::fabs(t.coef), &e2) == 0.5) {
+        for (int q = 0; q < pr.nc; ++q) p->terms[pr.c0 + q].coef *= t.coef;
+        t.coef = 1.0;
+      }
+    }
     p->prods.push_back(pr);
   }
   // C block lists for the scatter (products in increasing order per block).
@@ -312,9 +324,11 @@ int launch_gemm(int kind, const DevTables& d, const int grid_dims[3], int nprod,
   a.tickets = tickets;
   const unsigned grid = (unsigned)(units < sm_count[dev] ? units : sm_count[dev]);
   // A spans grid_dims[0] x grid_dims[1] blocks of ms x ks; B grid_dims[1] x grid_dims[2] of ks x ns
-  const bool tma =
-      make_tensor_map(&a.tmA, A, (long long)grid_dims[0] * ms, (long long)grid_dims[1] * ks, lda, fmm::BM, fmm::BK) &&
-      make_tensor_map(&a.tmB, B, (long long)grid_dims[1] * ks, (long long)grid_dims[2] * ns, ldb, fmm::TB_K, fmm::BN);
+  const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * ks,
+                  bn = (long long)grid_dims[2] * ns;
+  const bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
+                   make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
+                   make_tensor_map(&a.tmB2, B, ak, bn, ldb, fmm::TB_K, fmm::BN);
   {
     ProfScope ps(kind, st);
     if (tma)

@@ -34,10 +34,14 @@ constexpr int BK = 8;     // k depth of one operand stage
 constexpr int NPROD = 128;               // producer threads (warpgroup 0)
 constexpr int NCONS = 256;               // consumer threads (warpgroups 1, 2)
 constexpr int NTHREADS = NPROD + NCONS;  // 384
-constexpr int LDA_S = BM + 4;  // opA[k][m], padded: conflict-free fragment loads
-constexpr int LDB_S = BK + 4;  // opB[n][k]
-constexpr int NSTAGE = 4;      // operand stages (producer -> consumers)
-constexpr int NRAW = 8;        // thread-private raw term slots in flight per producer thread
+// Operand stages are dense: opA[k][m] (BK x BM) and opB[n][k] (BN x BK), exactly the
+// layout a TMA box writes, so single-term operands are copied straight into a stage.
+// (The consumers' FP64 fragment loads then see 4-way bank conflicts; shared-memory
+// bandwidth has room for that: measured no loss against padded rows.)
+constexpr int LDA_S = BM;      // opA[k][m]
+constexpr int LDB_S = BK;      // opB[n][k]
+constexpr int NSTAGE = 6;      // operand stages (producer -> consumers)
+constexpr int NRAW = 6;        // cp.async path: thread-private raw term slots in flight
 constexpr int EA = BM * BK / NPROD;  // A elements a producer thread stages per term (8)
 constexpr int EB = BN * BK / NPROD;  // B elements a producer thread stages per term (8)
 constexpr int OPA_SZ = BK * LDA_S;
@@ -50,9 +54,12 @@ constexpr int RAW_SZ = (EA + EB) * NPROD;
 constexpr int TB_K = BK + 2;
 constexpr int TRAW_A = BK * BM;
 constexpr int TRAW_SZ = TRAW_A + BN * TB_K;
-constexpr int NRAW_TMA = 7;
+constexpr int NRAW_TMA = 6;
+constexpr int NFOLD = NPROD - 32;  // folding threads: producer warps 1..3 (warp 0 issues TMA)
+constexpr int FPAIRS = (BM * BK / 2 + NFOLD - 1) / NFOLD;  // element pairs per folding thread per side
 constexpr unsigned TMA_BYTES_A = TRAW_A * sizeof(double);
-constexpr unsigned TMA_BYTES_B = BN * TB_K * sizeof(double);
+constexpr unsigned TMA_BYTES_B = BN * TB_K * sizeof(double);   // raw B box (k rounded down to even)
+constexpr unsigned TMA_BYTES_B8 = BN * BK * sizeof(double);    // direct B box
 static_assert((NSTAGE * STAGE_SZ * sizeof(double)) % 128 == 0, "raw slots must start 128-byte aligned");
 static_assert((TRAW_SZ * sizeof(double)) % 128 == 0, "TMA raw slots must be 128-byte aligned");
 static_assert((TRAW_A * sizeof(double)) % 128 == 0, "TMA B box must be 128-byte aligned");
@@ -62,8 +69,8 @@ constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_S
                                   (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long);
 constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
 constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
-constexpr int PROD_REGS = 72;
-constexpr int CONS_REGS = 216;
+constexpr int PROD_REGS = 120;
+constexpr int CONS_REGS = 176;
 static_assert(4 * 32 * PROD_REGS + 8 * 32 * CONS_REGS <= NTHREADS * 168, "register split exceeds the launch budget");
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ULL;  // bounded device-side waits give up after 4 s
 // try_wait suspends the waiting thread until the phase completes or this many ns pass,
@@ -87,8 +94,9 @@ enum Mode : int { MODE_ACCUM_C = 0, MODE_STORE_M = 1 };
 enum StatusBits : unsigned { STATUS_TICKET_TIMEOUT = 1u, STATUS_WAIT_TIMEOUT = 2u };
 
 struct GemmArgs {
-  CUtensorMap tmA;  // whole-matrix tensor maps (TMA path): A (m x k), B (k x n), FP64
-  CUtensorMap tmB;
+  CUtensorMap tmA;   // whole-matrix tensor maps (TMA path), FP64: A (m x k), box BM x BK
+  CUtensorMap tmB;   // B (k x n), box BK x BN (direct loads)
+  CUtensorMap tmB2;  // B (k x n), box (BK + 2) x BN (raw loads at even k)
   const double* A;
   long long lda;
   const double* B;
@@ -439,107 +447,179 @@ __device__ void producer(const GemmArgs& a, double* stages, double* raw, unsigne
 }
 
 // ------------------------------------------------------------------------------------
-// TMA producer: thread 0 issues one or two tensor copies per load unit into a raw slot
-// (completion counted in bytes on raw_full[slot]); all 128 producer threads then fold
-// the slot into the operand stage and release it on raw_empty[slot].
+// TMA producer.  Warp 0, lane 0 is the issuer: per k step it copies single-term
+// operands (coefficient 1, full k step, aligned) straight into the operand stage and
+// every term of a summed operand into a raw slot.  Warps 1..3 fold the raw slots of a
+// k step into registers (sum with coefficients, k tail masked) and store the result
+// into the stage once.  The stage's full barrier completes on the issuer's arrival
+// with its byte count plus one arrival per folding warp.
 // ------------------------------------------------------------------------------------
-__device__ __forceinline__ void issue_unit_tma(const GemmArgs& a, const LoadIter& it, double* raw_slot,
-                                               unsigned bar) {
-  const bool hasA = it.t < it.p.na, hasB = it.t < it.p.nb;
-  mbar_arrive_expect_tx(bar, (hasA ? TMA_BYTES_A : 0u) + (hasB ? TMA_BYTES_B : 0u));
-  const int k0 = it.s * BK;
-  if (hasA) {
-    // x = m coordinate: row * ms + m0 is even (ms is a multiple of 8, m0 of 128)
-    tma_load_2d(smem_u32(raw_slot), &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, bar);
+struct KStep {
+  bool dirA, dirB;  // operand copied straight into the stage
+  int T;            // raw loads for the summed operands
+};
+
+__device__ __forceinline__ KStep kstep_info(const GemmArgs& a, const LoadIter& it) {
+  KStep k;
+  const bool whole = (it.s + 1) * BK <= a.ks;
+  k.dirA = whole && it.p.na == 1 && it.ta.coef == 1.0;
+  k.dirB = whole && it.p.nb == 1 && it.tb.coef == 1.0 && ((it.tb.row * a.ks) & 1) == 0;
+  const int tA = k.dirA ? 0 : it.p.na, tB = k.dirB ? 0 : it.p.nb;
+  k.T = tA > tB ? tA : tB;
+  return k;
+}
+
+// Per-k-step iterator over (unit, product, k step); ta / tb hold the first A / B term.
+__device__ __forceinline__ void kiter_start(const GemmArgs& a, LoadIter& it, int nks) {
+  load_iter_start(a, it, nks);
+}
+__device__ __forceinline__ void kiter_next(const GemmArgs& a, LoadIter& it, int nks) {
+  it.t = 0;
+  if (++it.s < nks) return;
+  it.s = 0;
+  if (++it.r < it.w.r1) {
+    it.p = a.prods[it.r];
+    it.T = prod_T(it.p);
+    load_terms(a, it);
+    return;
   }
-  if (hasB) {
-    const int xk = it.tb.row * a.ks + k0;  // k coordinate; rounded down to even
-    tma_load_2d(smem_u32(raw_slot + TRAW_A), &a.tmB, xk & ~1, it.tb.col * a.ns + it.w.n0, bar);
+  it.u += gridDim.x;
+  if (it.u >= num_units(a)) {
+    it.valid = false;
+    return;
+  }
+  it.w = decode_unit(a, it.u);
+  it.r = it.w.r0;
+  it.p = a.prods[it.r];
+  it.T = prod_T(it.p);
+  load_terms(a, it);
+}
+
+__device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0,
+                           unsigned rfull0, unsigned rempty0, int nks) {
+  LoadIter it;
+  kiter_start(a, it, nks);
+  long long kc = 0, rc = 0;
+#pragma unroll 1
+  while (it.valid) {
+    const int stage = (int)(kc % NSTAGE);
+    double* opA = stages + (size_t)stage * STAGE_SZ;
+    const KStep ks = kstep_info(a, it);
+    const int k0 = it.s * BK;
+    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    const unsigned fb = full0 + 8 * stage;
+    mbar_arrive_expect_tx(fb, (ks.dirA ? TMA_BYTES_A : 0u) + (ks.dirB ? TMA_BYTES_B8 : 0u));
+    if (ks.dirA) tma_load_2d(smem_u32(opA), &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, fb);
+    if (ks.dirB)
+      tma_load_2d(smem_u32(opA + OPA_SZ), &a.tmB, it.tb.row * a.ks + k0, it.tb.col * a.ns + it.w.n0, fb);
+#pragma unroll 1
+    for (int t = 0; t < ks.T; ++t, ++rc) {
+      const int slot = (int)(rc % NRAW_TMA);
+      if (rc >= NRAW_TMA) mbar_wait(rempty0 + 8 * slot, (unsigned)(((rc / NRAW_TMA) - 1) & 1), a.status);
+      const bool hasA = !ks.dirA && t < it.p.na, hasB = !ks.dirB && t < it.p.nb;
+      const unsigned rb = rfull0 + 8 * slot;
+      double* rs = raw + (size_t)slot * TRAW_SZ;
+      mbar_arrive_expect_tx(rb, (hasA ? TMA_BYTES_A : 0u) + (hasB ? TMA_BYTES_B : 0u));
+      if (hasA) {
+        const Term tm = t == 0 ? it.ta : a.terms[it.p.a0 + t];
+        tma_load_2d(smem_u32(rs), &a.tmA, tm.row * a.ms + it.w.m0, tm.col * a.ks + k0, rb);
+      }
+      if (hasB) {
+        const Term tm = t == 0 ? it.tb : a.terms[it.p.b0 + t];
+        const int xk = tm.row * a.ks + k0;  // rounded down to even: TMA needs 16-byte x
+        tma_load_2d(smem_u32(rs + TRAW_A), &a.tmB2, xk & ~1, tm.col * a.ns + it.w.n0, rb);
+      }
+    }
+    ++kc;
+    kiter_next(a, it, nks);
   }
 }
 
-__device__ __forceinline__ void fold_unit_tma(const GemmArgs& a, const LoadIter& it, const double* raw_slot,
-                                              double* opA, double* opB, int pt) {
-  const int k0 = it.s * BK;
-  if (it.t < it.p.na) {
-    const double c = it.ta.coef;
-#pragma unroll
-    for (int e = 0; e < PA; ++e) {
-      const int q = e * NPROD + pt;
-      const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
-      double2 v = reinterpret_cast<const double2*>(raw_slot)[(kk * BM + mm) / 2];
-      if (k0 + kk >= a.ks) v = make_double2(0.0, 0.0);  // past the sub-block's k range
-      double2* dst = reinterpret_cast<double2*>(opA + kk * LDA_S + mm);
-      if (it.t == 0) {
-        *dst = make_double2(c * v.x, c * v.y);
-      } else {
-        const double2 o = *dst;
-        *dst = make_double2(fma(c, v.x, o.x), fma(c, v.y, o.y));
-      }
-    }
-  }
-  if (it.t < it.p.nb) {
-    const double c = it.tb.coef;
-    const int shift = (it.tb.row * a.ks) & 1;
-    const double* rb = raw_slot + TRAW_A;
-#pragma unroll
-    for (int e = 0; e < PB; ++e) {
-      const int q = e * NPROD + pt;
-      const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
-      double v0 = rb[nn * TB_K + kk + shift], v1 = rb[nn * TB_K + kk + 1 + shift];
-      if (k0 + kk >= a.ks) v0 = 0.0;
-      if (k0 + kk + 1 >= a.ks) v1 = 0.0;
-      double2* dst = reinterpret_cast<double2*>(opB + nn * LDB_S + kk);
-      if (it.t == 0) {
-        *dst = make_double2(c * v0, c * v1);
-      } else {
-        const double2 o = *dst;
-        *dst = make_double2(fma(c, v0, o.x), fma(c, v1, o.y));
-      }
-    }
-  }
-}
-
-__device__ void producer_tma(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0,
-                             unsigned rfull0, unsigned rempty0, int pt, int nks) {
-  LoadIter iss, con;
-  load_iter_start(a, iss, nks);
-  load_iter_start(a, con, nks);
-  if (pt == 0) {
+__device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, unsigned full0, unsigned empty0,
+                           unsigned rfull0, unsigned rempty0, int ft, int nks) {
+  LoadIter it;
+  kiter_start(a, it, nks);
+  long long kc = 0, rc = 0;
+  const int lane = ft & 31;
 #pragma unroll 1
-    for (int i = 0; i < NRAW_TMA - 1 && iss.valid; ++i) {
-      issue_unit_tma(a, iss, raw + (size_t)i * TRAW_SZ, rfull0 + 8 * i);
-      load_iter_next(a, iss, nks);
-    }
-  }
-  long long kc = 0;
-  long long unit = 0;
-#pragma unroll 1
-  while (con.valid) {
+  while (it.valid) {
     const int stage = (int)(kc % NSTAGE);
     double* opA = stages + (size_t)stage * STAGE_SZ;
     double* opB = opA + OPA_SZ;
-    if (con.t == 0) mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
-    const int slot = (int)(unit % NRAW_TMA);
-    mbar_wait(rfull0 + 8 * slot, (unsigned)((unit / NRAW_TMA) & 1), a.status);
-    fold_unit_tma(a, con, raw + (size_t)slot * TRAW_SZ, opA, opB, pt);
+    const KStep ks = kstep_info(a, it);
+    const int k0 = it.s * BK;
+    // Every folding warp waits for the stage to be released before it arrives on the
+    // stage's full barrier, even when it has nothing to fold: an arrival made earlier
+    // could land in the barrier's previous phase (whose issuer arrival and bytes may
+    // still be outstanding) and break that phase's transaction accounting.
+    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    if (ks.T > 0) {
+      double2 accA[FPAIRS], accB[FPAIRS];
+#pragma unroll 1
+      for (int t = 0; t < ks.T; ++t, ++rc) {
+        const int slot = (int)(rc % NRAW_TMA);
+        mbar_wait(rfull0 + 8 * slot, (unsigned)((rc / NRAW_TMA) & 1), a.status);
+        const double* rs = raw + (size_t)slot * TRAW_SZ;
+        if (!ks.dirA && t < it.p.na) {
+          const double c = (t == 0 ? it.ta : a.terms[it.p.a0 + t]).coef;
+#pragma unroll
+          for (int e = 0; e < FPAIRS; ++e) {
+            const int q = ft + e * NFOLD;
+            if (q < BM * BK / 2) {
+              const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+              double2 v = reinterpret_cast<const double2*>(rs)[(kk * BM + mm) / 2];
+              if (k0 + kk >= a.ks) v = make_double2(0.0, 0.0);
+              accA[e] = (t == 0) ? make_double2(c * v.x, c * v.y)
+                                 : make_double2(fma(c, v.x, accA[e].x), fma(c, v.y, accA[e].y));
+            }
+          }
+        }
+        if (!ks.dirB && t < it.p.nb) {
+          const Term tm = t == 0 ? it.tb : a.terms[it.p.b0 + t];
+          const double c = tm.coef;
+          const int shift = (tm.row * a.ks) & 1;
+          const double* rb = rs + TRAW_A;
+#pragma unroll
+          for (int e = 0; e < FPAIRS; ++e) {
+            const int q = ft + e * NFOLD;
+            if (q < BN * BK / 2) {
+              const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
+              double v0 = rb[nn * TB_K + kk + shift], v1 = rb[nn * TB_K + kk + 1 + shift];
+              if (k0 + kk >= a.ks) v0 = 0.0;
+              if (k0 + kk + 1 >= a.ks) v1 = 0.0;
+              accB[e] = (t == 0) ? make_double2(c * v0, c * v1)
+                                 : make_double2(fma(c, v0, accB[e].x), fma(c, v1, accB[e].y));
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(rempty0 + 8 * slot);
+      }
+      if (!ks.dirA) {
+#pragma unroll
+        for (int e = 0; e < FPAIRS; ++e) {
+          const int q = ft + e * NFOLD;
+          if (q < BM * BK / 2) {
+            const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+            *reinterpret_cast<double2*>(opA + kk * LDA_S + mm) = accA[e];
+          }
+        }
+      }
+      if (!ks.dirB) {
+#pragma unroll
+        for (int e = 0; e < FPAIRS; ++e) {
+          const int q = ft + e * NFOLD;
+          if (q < BN * BK / 2) {
+            const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
+            *reinterpret_cast<double2*>(opB + nn * LDB_S + kk) = accB[e];
+          }
+        }
+      }
+    }
     __syncwarp();
-    if ((pt & 31) == 0) mbar_arrive(rempty0 + 8 * slot);
-    if (con.t == con.T - 1) {
-      if ((pt & 31) == 0) mbar_arrive(full0 + 8 * stage);
-      ++kc;
-    }
-    if (pt == 0 && iss.valid) {
-      // unit + NRAW_TMA - 1 reuses the slot of unit - 1: wait until every producer warp
-      // has folded it
-      const long long nu = unit + NRAW_TMA - 1;
-      const int islot = (int)(nu % NRAW_TMA);
-      if (unit >= 1) mbar_wait(rempty0 + 8 * islot, (unsigned)(((unit - 1) / NRAW_TMA) & 1), a.status);
-      issue_unit_tma(a, iss, raw + (size_t)islot * TRAW_SZ, rfull0 + 8 * islot);
-      load_iter_next(a, iss, nks);
-    }
-    ++unit;
-    load_iter_next(a, con, nks);
+    if (lane == 0) mbar_arrive(full0 + 8 * stage);
+    ++kc;
+    kiter_next(a, it, nks);
   }
 }
 
@@ -692,13 +772,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(full0 + 8 * s, NPROD / 32);
+      // full: TMA path = issuer (1) + folding warps; cp.async path = the 4 producer warps
+      mbar_init(full0 + 8 * s, TMA ? 1 + NFOLD / 32 : NPROD / 32);
       mbar_init(empty0 + 8 * s, NCONS / 32);
     }
     if (TMA) {
       for (int s = 0; s < NRAW_TMA; ++s) {
         mbar_init(rfull0 + 8 * s, 1);
-        mbar_init(rempty0 + 8 * s, NPROD / 32);
+        mbar_init(rempty0 + 8 * s, NFOLD / 32);
       }
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -707,10 +788,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
   const int nks = (a.ks + BK - 1) / BK;
   if (tid < NPROD) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
-    if (TMA)
-      producer_tma(a, stages, raw, full0, empty0, rfull0, rempty0, tid, nks);
-    else
+    if (TMA) {
+      if (tid == 0)
+        tma_issuer(a, stages, raw, full0, empty0, rfull0, rempty0, nks);
+      else if (tid >= 32)
+        tma_folder(a, stages, raw, full0, empty0, rfull0, rempty0, tid - 32, nks);
+    } else {
       producer(a, stages, raw, full0, empty0, tid, nks);
+    }
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
     consumer(a, stages, full0, empty0, tid - NPROD, nks);

@@ -20,7 +20,7 @@ import numpy as np
 from . import algebra
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
-LIB_PATH = os.path.join(LIB_DIR, "libfmm_b200.so")
+LIB_PATH = os.environ.get("FMM_B200_LIB") or os.path.join(LIB_DIR, "libfmm_b200.so")
 
 PACK_TYPES = {"abc": 0, "ab": 1, "naive": 2}
 
