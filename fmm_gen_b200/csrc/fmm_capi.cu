@@ -72,6 +72,10 @@ struct DevTables {
   int* cblk = nullptr;
   int* ent_r = nullptr;
   double* ent_w = nullptr;
+  fmm::Prod* prods_ps = nullptr;  // products over pre-summed operands (one A and one B term each)
+  fmm::Term* terms_ps = nullptr;
+  int* plistA = nullptr;          // products whose A operand is pre-summed, in slot order
+  int* plistB = nullptr;
   bool ready = false;
 };
 
@@ -87,6 +91,11 @@ struct fmm_plan {
   std::vector<int> ent_r;
   std::vector<double> ent_w;
   int n_cblk = 0;
+  // Pre-summed form: each product's A operand is either its single A block (src 0) or
+  // slot j of the workspace S (src 1) that holds sum_i U[i,r] A_i; likewise for B / T.
+  std::vector<fmm::Prod> prods_ps;
+  std::vector<fmm::Term> terms_ps;
+  std::vector<int> plistA, plistB;
   std::mutex mu;
   DevTables dev[kMaxDevices];
 };
@@ -124,6 +133,18 @@ int upload_tables(fmm_plan* p, DevTables& d) {
     FMM_CUDA_TRY(cudaMemcpy(d.ent_r, p->ent_r.data(), sizeof(int) * p->ent_r.size(), cudaMemcpyHostToDevice));
     FMM_CUDA_TRY(cudaMemcpy(d.ent_w, p->ent_w.data(), sizeof(double) * p->ent_w.size(), cudaMemcpyHostToDevice));
   }
+  FMM_CUDA_TRY(cudaMalloc(&d.prods_ps, sizeof(fmm::Prod) * p->prods_ps.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.terms_ps, sizeof(fmm::Term) * p->terms_ps.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.plistA, sizeof(int) * (p->plistA.size() + 1)));
+  FMM_CUDA_TRY(cudaMalloc(&d.plistB, sizeof(int) * (p->plistB.size() + 1)));
+  FMM_CUDA_TRY(cudaMemcpy(d.prods_ps, p->prods_ps.data(), sizeof(fmm::Prod) * p->prods_ps.size(),
+                          cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemcpy(d.terms_ps, p->terms_ps.data(), sizeof(fmm::Term) * p->terms_ps.size(),
+                          cudaMemcpyHostToDevice));
+  if (!p->plistA.empty())
+    FMM_CUDA_TRY(cudaMemcpy(d.plistA, p->plistA.data(), sizeof(int) * p->plistA.size(), cudaMemcpyHostToDevice));
+  if (!p->plistB.empty())
+    FMM_CUDA_TRY(cudaMemcpy(d.plistB, p->plistB.data(), sizeof(int) * p->plistB.size(), cudaMemcpyHostToDevice));
   d.ready = true;
   return FMM_OK;
 }
@@ -169,7 +190,7 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
           delete p;
           return FMM_E_PLAN;
         }
-        p->terms.push_back(fmm::Term{rows[pos], cols[pos], coefs[pos]});
+        p->terms.push_back(fmm::Term{rows[pos], cols[pos], coefs[pos], 0, 0});
       }
     }
     // A single operand term whose coefficient is a power of two moves its coefficient
@@ -206,6 +227,32 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
       p->ent_w.push_back(e.second);
     }
     ++p->n_cblk;
+  }
+  for (int r = 0; r < rank; ++r) {
+    const fmm::Prod& pr = p->prods[r];
+    fmm::Prod q{};
+    q.a0 = (int)p->terms_ps.size();
+    q.na = 1;
+    const fmm::Term& ta = p->terms[pr.a0];
+    if (pr.na == 1 && ta.coef == 1.0) {
+      p->terms_ps.push_back(ta);
+    } else {
+      p->terms_ps.push_back(fmm::Term{0, (int)p->plistA.size(), 1.0, 1, 0});
+      p->plistA.push_back(r);
+    }
+    q.b0 = (int)p->terms_ps.size();
+    q.nb = 1;
+    const fmm::Term& tb = p->terms[pr.b0];
+    if (pr.nb == 1 && tb.coef == 1.0) {
+      p->terms_ps.push_back(tb);
+    } else {
+      p->terms_ps.push_back(fmm::Term{0, (int)p->plistB.size(), 1.0, 1, 0});
+      p->plistB.push_back(r);
+    }
+    q.c0 = (int)p->terms_ps.size();
+    q.nc = pr.nc;
+    for (int c = 0; c < pr.nc; ++c) p->terms_ps.push_back(p->terms[pr.c0 + c]);
+    p->prods_ps.push_back(q);
   }
   *out = p;
   return FMM_OK;
@@ -249,6 +296,14 @@ int configure_kernel(int* dev_out) {
         g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
     FMM_CUDA_TRY(cudaDeviceGetAttribute(&sm_count[dev], cudaDevAttrMultiProcessorCount, dev));
+    // Workspaces come from the device's stream-ordered pool; keep freed blocks mapped
+    // instead of returning them to the driver at every synchronisation, so repeated
+    // calls do not pay for mapping gigabytes of workspace again.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      cuuint64_t keep = ~0ULL;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     FMM_CUDA_TRY(cudaMalloc(&dev_status[dev], sizeof(unsigned)));
     FMM_CUDA_TRY(cudaMemset(dev_status[dev], 0, sizeof(unsigned)));
     smem_configured[dev] = true;
@@ -285,9 +340,20 @@ int choose_chunks(int ntiles, int nprod, int nsm) {
 }
 
 // Launch the persistent DMMA GEMM over sub-blocks of size ms x ks x ns.
-int launch_gemm(int kind, const DevTables& d, const int grid_dims[3], int nprod, int mode, const double* A,
-                long long lda, const double* B, long long ldb, double* C, long long ldc, double* M, long long ldm,
-                long long m_stride, int ms, int ns, int ks, cudaStream_t st) {
+// Workspaces of pre-summed operands (slot j of S: ms x ks, of T: ks x ns, block columns).
+struct PresumOps {
+  const double* S = nullptr;
+  long long ldS = 0;
+  int nslotA = 0;
+  const double* T = nullptr;
+  long long ldT = 0;
+  int nslotB = 0;
+};
+
+int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
+                int mode, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
+                double* C, long long ldc, double* M, long long ldm, long long m_stride, int ms, int ns, int ks,
+                cudaStream_t st) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
   int dev = 0;
   int rc = configure_kernel(&dev);
@@ -305,8 +371,12 @@ int launch_gemm(int kind, const DevTables& d, const int grid_dims[3], int nprod,
   a.ms = ms;
   a.ns = ns;
   a.ks = ks;
-  a.prods = d.prods;
-  a.terms = d.terms;
+  a.prods = prods;
+  a.terms = terms;
+  a.Aw = ps.S ? ps.S : A;
+  a.ldaw = ps.S ? ps.ldS : lda;
+  a.Bw = ps.T ? ps.T : B;
+  a.ldbw = ps.T ? ps.ldT : ldb;
   a.nprod = nprod;
   a.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
   a.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
@@ -326,9 +396,22 @@ int launch_gemm(int kind, const DevTables& d, const int grid_dims[3], int nprod,
   // A spans grid_dims[0] x grid_dims[1] blocks of ms x ks; B grid_dims[1] x grid_dims[2] of ks x ns
   const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * ks,
                   bn = (long long)grid_dims[2] * ns;
-  const bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
-                   make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
-                   make_tensor_map(&a.tmB2, B, ak, bn, ldb, fmm::TB_K, fmm::BN);
+  bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
+             make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
+             make_tensor_map(&a.tmB2, B, ak, bn, ldb, fmm::TB_K, fmm::BN);
+  if (tma) {
+    if (ps.S && ps.nslotA > 0)
+      tma = make_tensor_map(&a.tmAw, ps.S, ms, (long long)ps.nslotA * ks, ps.ldS, fmm::BM, fmm::BK);
+    else
+      a.tmAw = a.tmA;
+  }
+  if (tma) {
+    if (ps.T && ps.nslotB > 0)
+      tma = make_tensor_map(&a.tmBw, ps.T, ks, (long long)ps.nslotB * ns, ps.ldT, fmm::BK, fmm::BN) &&
+            make_tensor_map(&a.tmBw2, ps.T, ks, (long long)ps.nslotB * ns, ps.ldT, fmm::TB_K, fmm::BN);
+    else
+      a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
+  }
   {
     ProfScope ps(kind, st);
     if (tma)
@@ -353,7 +436,8 @@ int plain_gemm(int m, int n, int k, const double* A, long long lda, const double
   DevTables* d = nullptr;
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
-  return launch_gemm(K_GEMM_CLASSICAL, *d, kUnitGrid, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, m, n, k, st);
+  return launch_gemm(K_GEMM_CLASSICAL, d->prods, d->terms, kUnitGrid, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb,
+                     PresumOps{}, C, ldc, nullptr, 0, 0, m, n, k, st);
 }
 
 int grid_for(long long total, int threads) {
@@ -384,6 +468,58 @@ int peel(int m, int n, int k, const double* A, long long lda, const double* B, l
   return FMM_OK;
 }
 
+// Pre-summing pays off once a product's k depth amortises the extra pass over HBM
+// (each operand sum is written once and read by every tile that uses it).
+bool use_presum(const fmm_plan* plan, int ms, int ns, int ks) {
+  if (plan->plistA.empty() && plan->plistB.empty()) return false;
+  return (long long)ms * ns >= (1LL << 20) && ks >= 256;
+}
+
+int presum(const DevTables& d, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
+           int ms, int ns, int ks, cudaStream_t st) {
+  if (ps.nslotA > 0) {
+    fmm::LincombArgs la{};
+    la.X = A;
+    la.ldx = lda;
+    la.rows = ms;
+    la.cols = ks;
+    la.blk_row_stride = ms;
+    la.blk_col_stride = ks;
+    la.out = const_cast<double*>(ps.S);
+    la.ldo = ps.ldS;
+    la.out_stride = ps.ldS * ks;
+    la.prods = d.prods;
+    la.terms = d.terms;
+    la.plist = d.plistA;
+    la.side = 0;
+    const dim3 g((unsigned)grid_for((long long)(ms + 1) / 2 * ks, 256), (unsigned)ps.nslotA);
+    ProfScope pf(K_LINCOMB, st);
+    fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(la);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  if (ps.nslotB > 0) {
+    fmm::LincombArgs lb{};
+    lb.X = B;
+    lb.ldx = ldb;
+    lb.rows = ks;
+    lb.cols = ns;
+    lb.blk_row_stride = ks;
+    lb.blk_col_stride = ns;
+    lb.out = const_cast<double*>(ps.T);
+    lb.ldo = ps.ldT;
+    lb.out_stride = ps.ldT * ns;
+    lb.prods = d.prods;
+    lb.terms = d.terms;
+    lb.plist = d.plistB;
+    lb.side = 1;
+    const dim3 g((unsigned)grid_for((long long)(ks + 1) / 2 * ns, 256), (unsigned)ps.nslotB);
+    ProfScope pf(K_LINCOMB, st);
+    fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(lb);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
 int check_args(int m, int n, int k, const void* A, long long lda, const void* B, long long ldb, const void* C,
                long long ldc) {
   if (m < 0 || n < 0 || k < 0) return FMM_E_INVALID;
@@ -409,7 +545,32 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   const int R = plan->rank;
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
-      rc = launch_gemm(K_GEMM_FMM, *d, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+      const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
+      if (use_presum(plan, ms, ns, ks)) {
+        // U/V sums formed once per product in HBM (bandwidth-bound), then every
+        // product reads single operands; products scattered into C in the epilogue.
+        PresumOps ps;
+        const long long ldT = ks + (ks & 1);
+        const size_t sbytes = sizeof(double) * (size_t)ms * ks * nA;
+        const size_t tbytes = sizeof(double) * (size_t)ldT * ns * nB;
+        char* ws = nullptr;
+        FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, sbytes + tbytes + 16, st));
+        ps.S = reinterpret_cast<double*>(ws);
+        ps.ldS = ms;
+        ps.nslotA = nA;
+        ps.T = reinterpret_cast<double*>(ws + sbytes);
+        ps.ldT = ldT;
+        ps.nslotB = nB;
+        rc = presum(*d, A, lda, B, ldb, ps, ms, ns, ks, st);
+        if (rc == FMM_OK)
+          rc = launch_gemm(K_GEMM_FMM, d->prods_ps, d->terms_ps, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
+                           ps, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+        cudaError_t fe = cudaFreeAsync(ws, st);
+        if (rc == FMM_OK) rc = cuda_status(fe);
+      } else {
+        rc = launch_gemm(K_GEMM_FMM, d->prods, d->terms, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
+                         PresumOps{}, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+      }
       if (rc != FMM_OK) return rc;
     } else {
       const long long mstride = (long long)ms * ns;
@@ -423,7 +584,8 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
       FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes + s_bytes + t_bytes, st));
       double* M = reinterpret_cast<double*>(ws);
       if (pack == FMM_PACK_AB) {
-        rc = launch_gemm(K_GEMM_FMM, *d, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb, C, ldc, M, ms, mstride, ms, ns, ks, st);
+        rc = launch_gemm(K_GEMM_FMM, d->prods, d->terms, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb,
+                         PresumOps{}, C, ldc, M, ms, mstride, ms, ns, ks, st);
       } else {
         double* S = reinterpret_cast<double*>(ws + bytes);
         double* T = reinterpret_cast<double*>(ws + bytes + s_bytes);
@@ -440,7 +602,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         la.prods = d->prods;
         la.terms = d->terms;
         la.side = 0;
-        la.r_begin = 0;
+        la.plist = nullptr;
         const dim3 ga((unsigned)grid_for((long long)ms * ks, 256), (unsigned)R);
         {
           ProfScope ps(K_LINCOMB, st);
@@ -470,9 +632,9 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
           DevTables* dc = nullptr;
           rc = device_tables(classical_plan(), &dc);
           for (int r = 0; rc == FMM_OK && r < R; ++r) {
-            rc = launch_gemm(K_GEMM_FMM, *dc, kUnitGrid, 1, fmm::MODE_STORE_M, S + (long long)r * ms * ks, ms,
-                             T + (long long)r * ks * ns, ks, nullptr, 0, M + (long long)r * mstride, ms, 0, ms, ns,
-                             ks, st);
+            rc = launch_gemm(K_GEMM_FMM, dc->prods, dc->terms, kUnitGrid, 1, fmm::MODE_STORE_M,
+                             S + (long long)r * ms * ks, ms, T + (long long)r * ks * ns, ks, PresumOps{}, nullptr, 0,
+                             M + (long long)r * mstride, ms, 0, ms, ns, ks, st);
           }
         }
       }
@@ -573,6 +735,10 @@ int fmm_plan_destroy(fmm_plan* plan) {
     cudaFree(d.cblk);
     cudaFree(d.ent_r);
     cudaFree(d.ent_w);
+    cudaFree(d.prods_ps);
+    cudaFree(d.terms_ps);
+    cudaFree(d.plistA);
+    cudaFree(d.plistB);
   }
   delete plan;
   return FMM_OK;

@@ -31,9 +31,10 @@ namespace fmm {
 constexpr int BM = 128;   // CTA tile rows (m)
 constexpr int BN = 128;   // CTA tile columns (n)
 constexpr int BK = 8;     // k depth of one operand stage
-constexpr int NPROD = 128;               // producer threads (warpgroup 0)
-constexpr int NCONS = 256;               // consumer threads (warpgroups 1, 2)
-constexpr int NTHREADS = NPROD + NCONS;  // 384
+constexpr int NPROD = 256;               // producer threads (warpgroups 0, 1)
+constexpr int NCONS = 256;               // consumer threads (warpgroups 2, 3)
+constexpr int NTHREADS = NPROD + NCONS;  // 512
+constexpr int LAUNCH_REGS = 65536 / NTHREADS;  // registers per thread at launch (128)
 // Operand stages are dense: opA[k][m] (BK x BM) and opB[n][k] (BN x BK), exactly the
 // layout a TMA box writes, so single-term operands are copied straight into a stage.
 // (The consumers' FP64 fragment loads then see 4-way bank conflicts; shared-memory
@@ -55,8 +56,9 @@ constexpr int TB_K = BK + 2;
 constexpr int TRAW_A = BK * BM;
 constexpr int TRAW_SZ = TRAW_A + BN * TB_K;
 constexpr int NRAW_TMA = 6;
-constexpr int NFOLD = NPROD - 32;  // folding threads: producer warps 1..3 (warp 0 issues TMA)
-constexpr int FPAIRS = (BM * BK / 2 + NFOLD - 1) / NFOLD;  // element pairs per folding thread per side
+constexpr int NFOLD = NPROD - 32;  // folding threads: producer warps 1..7 (warp 0 issues TMA)
+constexpr int FPAIRS = (BM * BK / 2 + NFOLD - 1) / NFOLD;  // A element pairs per folding thread
+constexpr int FELEMS = (BN * BK + NFOLD - 1) / NFOLD;      // B elements per folding thread
 constexpr unsigned TMA_BYTES_A = TRAW_A * sizeof(double);
 constexpr unsigned TMA_BYTES_B = BN * TB_K * sizeof(double);   // raw B box (k rounded down to even)
 constexpr unsigned TMA_BYTES_B8 = BN * BK * sizeof(double);    // direct B box
@@ -65,13 +67,22 @@ static_assert((TRAW_SZ * sizeof(double)) % 128 == 0, "TMA raw slots must be 128-
 static_assert((TRAW_A * sizeof(double)) % 128 == 0, "TMA B box must be 128-byte aligned");
 constexpr size_t SMEM_BYTES_CPASYNC =
     (size_t)(NSTAGE * STAGE_SZ + NRAW * RAW_SZ) * sizeof(double) + 2 * NSTAGE * sizeof(unsigned long long);
+// What the folding warps need to know about a raw slot, written by the issuer before
+// the slot's TMA copies (published by the release of its arrive.expect_tx).
+struct SlotMeta {
+  double ca, cb;  // coefficients of the staged A and B terms
+  int shift;      // B box starts one k before the term's first k
+  int pad[3];
+};
 constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_SZ) * sizeof(double) +
+                                  NRAW_TMA * sizeof(SlotMeta) +
                                   (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long);
 constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
 constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
-constexpr int PROD_REGS = 120;
+constexpr int PROD_REGS = 80;
 constexpr int CONS_REGS = 176;
-static_assert(4 * 32 * PROD_REGS + 8 * 32 * CONS_REGS <= NTHREADS * 168, "register split exceeds the launch budget");
+static_assert(NPROD * PROD_REGS + NCONS * CONS_REGS <= NTHREADS * LAUNCH_REGS,
+              "register split exceeds the launch budget");
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ULL;  // bounded device-side waits give up after 4 s
 // try_wait suspends the waiting thread until the phase completes or this many ns pass,
 // so waiting warps do not take issue slots from the warps they wait for.
@@ -81,6 +92,8 @@ struct Term {
   int row;      // global block row in the composed grid
   int col;      // global block column
   double coef;  // coefficient
+  int src;      // A/B terms: 0 = the operand matrix, 1 = the pre-summed workspace (S / T)
+  int pad;
 };
 
 struct Prod {
@@ -97,10 +110,17 @@ struct GemmArgs {
   CUtensorMap tmA;   // whole-matrix tensor maps (TMA path), FP64: A (m x k), box BM x BK
   CUtensorMap tmB;   // B (k x n), box BK x BN (direct loads)
   CUtensorMap tmB2;  // B (k x n), box (BK + 2) x BN (raw loads at even k)
+  CUtensorMap tmAw;  // the same three for the pre-summed workspaces S (A side) and T (B side)
+  CUtensorMap tmBw;
+  CUtensorMap tmBw2;
   const double* A;
   long long lda;
   const double* B;
   long long ldb;
+  const double* Aw;  // pre-summed operands: S holds one ms x ks block per slot (block column),
+  long long ldaw;    // T one ks x ns block per slot (block column); terms with src = 1 point here
+  const double* Bw;
+  long long ldbw;
   double* C;      // MODE_ACCUM_C: C blocks receive C_l += w * M_r
   long long ldc;
   double* M;      // MODE_STORE_M: product r stored at M + r * m_stride (ld = ldm)
@@ -325,9 +345,11 @@ constexpr int PB = EB / 2;
 __device__ __forceinline__ void issue_unit(const GemmArgs& a, const LoadIter& it, double* raw_slot, int pt) {
   const unsigned sbase = smem_u32(raw_slot);
   if (it.t < it.p.na) {
-    const long long off = (long long)it.ta.row * a.ms + (long long)it.ta.col * a.ks * a.lda;
-    const double* base = a.A + off;
-    const bool al16 = ((off & 1) == 0) && ((a.lda & 1) == 0) && ((reinterpret_cast<uintptr_t>(a.A) & 15) == 0);
+    const double* M0 = it.ta.src ? a.Aw : a.A;
+    const long long ld = it.ta.src ? a.ldaw : a.lda;
+    const long long off = (long long)it.ta.row * a.ms + (long long)it.ta.col * a.ks * ld;
+    const double* base = M0 + off;
+    const bool al16 = ((off & 1) == 0) && ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(M0) & 15) == 0);
 #pragma unroll
     for (int e = 0; e < PA; ++e) {
       const int q = e * NPROD + pt;        // pair index
@@ -336,18 +358,20 @@ __device__ __forceinline__ void issue_unit(const GemmArgs& a, const LoadIter& it
       const unsigned dst = sbase + (unsigned)(q * 16);
       if (al16) {
         const int nb = (gk < a.ks) ? ((gm + 1 < a.ms) ? 16 : (gm < a.ms ? 8 : 0)) : 0;
-        cp_async16(dst, nb ? base + gm + (long long)gk * a.lda : a.A, nb);
+        cp_async16(dst, nb ? base + gm + (long long)gk * ld : M0, nb);
       } else {
         const bool v0 = (gk < a.ks) && (gm < a.ms), v1 = (gk < a.ks) && (gm + 1 < a.ms);
-        cp_async8(dst, v0 ? base + gm + (long long)gk * a.lda : a.A, v0 ? 8 : 0);
-        cp_async8(dst + 8, v1 ? base + gm + 1 + (long long)gk * a.lda : a.A, v1 ? 8 : 0);
+        cp_async8(dst, v0 ? base + gm + (long long)gk * ld : M0, v0 ? 8 : 0);
+        cp_async8(dst + 8, v1 ? base + gm + 1 + (long long)gk * ld : M0, v1 ? 8 : 0);
       }
     }
   }
   if (it.t < it.p.nb) {
-    const long long off = (long long)it.tb.row * a.ks + (long long)it.tb.col * a.ns * a.ldb;
-    const double* base = a.B + off;
-    const bool al16 = ((off & 1) == 0) && ((a.ldb & 1) == 0) && ((reinterpret_cast<uintptr_t>(a.B) & 15) == 0);
+    const double* M0 = it.tb.src ? a.Bw : a.B;
+    const long long ld = it.tb.src ? a.ldbw : a.ldb;
+    const long long off = (long long)it.tb.row * a.ks + (long long)it.tb.col * a.ns * ld;
+    const double* base = M0 + off;
+    const bool al16 = ((off & 1) == 0) && ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(M0) & 15) == 0);
 #pragma unroll
     for (int e = 0; e < PB; ++e) {
       const int q = e * NPROD + pt;
@@ -356,11 +380,11 @@ __device__ __forceinline__ void issue_unit(const GemmArgs& a, const LoadIter& it
       const unsigned dst = sbase + (unsigned)((PA * NPROD + q) * 16);
       if (al16) {
         const int nb = (gn < a.ns) ? ((gk + 1 < a.ks) ? 16 : (gk < a.ks ? 8 : 0)) : 0;
-        cp_async16(dst, nb ? base + gk + (long long)gn * a.ldb : a.B, nb);
+        cp_async16(dst, nb ? base + gk + (long long)gn * ld : M0, nb);
       } else {
         const bool v0 = (gn < a.ns) && (gk < a.ks), v1 = (gn < a.ns) && (gk + 1 < a.ks);
-        cp_async8(dst, v0 ? base + gk + (long long)gn * a.ldb : a.B, v0 ? 8 : 0);
-        cp_async8(dst + 8, v1 ? base + gk + 1 + (long long)gn * a.ldb : a.B, v1 ? 8 : 0);
+        cp_async8(dst, v0 ? base + gk + (long long)gn * ld : M0, v0 ? 8 : 0);
+        cp_async8(dst + 8, v1 ? base + gk + 1 + (long long)gn * ld : M0, v1 ? 8 : 0);
       }
     }
   }
@@ -495,8 +519,8 @@ __device__ __forceinline__ void kiter_next(const GemmArgs& a, LoadIter& it, int 
   load_terms(a, it);
 }
 
-__device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0,
-                           unsigned rfull0, unsigned rempty0, int nks) {
+__device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, SlotMeta* meta, unsigned full0,
+                           unsigned empty0, unsigned rfull0, unsigned rempty0, int nks) {
   LoadIter it;
   kiter_start(a, it, nks);
   long long kc = 0, rc = 0;
@@ -509,9 +533,12 @@ __device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, unsig
     mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
     const unsigned fb = full0 + 8 * stage;
     mbar_arrive_expect_tx(fb, (ks.dirA ? TMA_BYTES_A : 0u) + (ks.dirB ? TMA_BYTES_B8 : 0u));
-    if (ks.dirA) tma_load_2d(smem_u32(opA), &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, fb);
+    if (ks.dirA)
+      tma_load_2d(smem_u32(opA), it.ta.src ? &a.tmAw : &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0,
+                  fb);
     if (ks.dirB)
-      tma_load_2d(smem_u32(opA + OPA_SZ), &a.tmB, it.tb.row * a.ks + k0, it.tb.col * a.ns + it.w.n0, fb);
+      tma_load_2d(smem_u32(opA + OPA_SZ), it.tb.src ? &a.tmBw : &a.tmB, it.tb.row * a.ks + k0,
+                  it.tb.col * a.ns + it.w.n0, fb);
 #pragma unroll 1
     for (int t = 0; t < ks.T; ++t, ++rc) {
       const int slot = (int)(rc % NRAW_TMA);
@@ -519,24 +546,60 @@ __device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, unsig
       const bool hasA = !ks.dirA && t < it.p.na, hasB = !ks.dirB && t < it.p.nb;
       const unsigned rb = rfull0 + 8 * slot;
       double* rs = raw + (size_t)slot * TRAW_SZ;
+      const Term tA = hasA ? (t == 0 ? it.ta : a.terms[it.p.a0 + t]) : Term{0, 0, 0.0, 0, 0};
+      const Term tB = hasB ? (t == 0 ? it.tb : a.terms[it.p.b0 + t]) : Term{0, 0, 0.0, 0, 0};
+      const int xk = tB.row * a.ks + k0;  // B box k coordinate, rounded down to even: TMA needs 16-byte x
+      meta[slot].ca = tA.coef;
+      meta[slot].cb = tB.coef;
+      meta[slot].shift = xk & 1;
       mbar_arrive_expect_tx(rb, (hasA ? TMA_BYTES_A : 0u) + (hasB ? TMA_BYTES_B : 0u));
-      if (hasA) {
-        const Term tm = t == 0 ? it.ta : a.terms[it.p.a0 + t];
-        tma_load_2d(smem_u32(rs), &a.tmA, tm.row * a.ms + it.w.m0, tm.col * a.ks + k0, rb);
-      }
-      if (hasB) {
-        const Term tm = t == 0 ? it.tb : a.terms[it.p.b0 + t];
-        const int xk = tm.row * a.ks + k0;  // rounded down to even: TMA needs 16-byte x
-        tma_load_2d(smem_u32(rs + TRAW_A), &a.tmB2, xk & ~1, tm.col * a.ns + it.w.n0, rb);
-      }
+      if (hasA)
+        tma_load_2d(smem_u32(rs), tA.src ? &a.tmAw : &a.tmA, tA.row * a.ms + it.w.m0, tA.col * a.ks + k0, rb);
+      if (hasB) tma_load_2d(smem_u32(rs + TRAW_A), tB.src ? &a.tmBw2 : &a.tmB2, xk & ~1, tB.col * a.ns + it.w.n0, rb);
     }
     ++kc;
     kiter_next(a, it, nks);
   }
 }
 
-__device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, unsigned full0, unsigned empty0,
-                           unsigned rfull0, unsigned rempty0, int ft, int nks) {
+// One raw slot folded into the running sums.  A: element pairs along m (16-byte
+// loads, conflict-free); B: single elements with consecutive k per lane, which spreads
+// the 80-byte box columns over all banks.  The k tail of a sub-block (k >= ks) only
+// exists on a product's last k step and is masked there.
+template <bool TAIL>
+__device__ __forceinline__ void fold_slot(const double* rs, const SlotMeta& m, bool hasA, bool hasB, bool first,
+                                          double2 (&accA)[FPAIRS], double (&accB)[FELEMS], int ft, int kvalid) {
+  if (hasA) {
+    const double c = m.ca;
+#pragma unroll
+    for (int e = 0; e < FPAIRS; ++e) {
+      const int q = ft + e * NFOLD;
+      if (q < BM * BK / 2) {
+        const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
+        double2 v = reinterpret_cast<const double2*>(rs)[(kk * BM + mm) / 2];
+        if (TAIL && kk >= kvalid) v = make_double2(0.0, 0.0);
+        accA[e] = first ? make_double2(c * v.x, c * v.y) : make_double2(fma(c, v.x, accA[e].x), fma(c, v.y, accA[e].y));
+      }
+    }
+  }
+  if (hasB) {
+    const double c = m.cb;
+    const double* rb = rs + TRAW_A + m.shift;
+#pragma unroll
+    for (int e = 0; e < FELEMS; ++e) {
+      const int q = ft + e * NFOLD;
+      if (q < BN * BK) {
+        const int kk = q % BK, nn = q / BK;
+        double v = rb[nn * TB_K + kk];
+        if (TAIL && kk >= kvalid) v = 0.0;
+        accB[e] = first ? c * v : fma(c, v, accB[e]);
+      }
+    }
+  }
+}
+
+__device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, const SlotMeta* meta,
+                           unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft, int nks) {
   LoadIter it;
   kiter_start(a, it, nks);
   long long kc = 0, rc = 0;
@@ -547,51 +610,25 @@ __device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw,
     double* opA = stages + (size_t)stage * STAGE_SZ;
     double* opB = opA + OPA_SZ;
     const KStep ks = kstep_info(a, it);
-    const int k0 = it.s * BK;
+    const int kvalid = a.ks - it.s * BK;  // valid k values in this step (>= BK except at the tail)
     // Every folding warp waits for the stage to be released before it arrives on the
     // stage's full barrier, even when it has nothing to fold: an arrival made earlier
     // could land in the barrier's previous phase (whose issuer arrival and bytes may
     // still be outstanding) and break that phase's transaction accounting.
     mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
     if (ks.T > 0) {
-      double2 accA[FPAIRS], accB[FPAIRS];
+      double2 accA[FPAIRS];
+      double accB[FELEMS];
 #pragma unroll 1
       for (int t = 0; t < ks.T; ++t, ++rc) {
         const int slot = (int)(rc % NRAW_TMA);
         mbar_wait(rfull0 + 8 * slot, (unsigned)((rc / NRAW_TMA) & 1), a.status);
         const double* rs = raw + (size_t)slot * TRAW_SZ;
-        if (!ks.dirA && t < it.p.na) {
-          const double c = (t == 0 ? it.ta : a.terms[it.p.a0 + t]).coef;
-#pragma unroll
-          for (int e = 0; e < FPAIRS; ++e) {
-            const int q = ft + e * NFOLD;
-            if (q < BM * BK / 2) {
-              const int mm = 2 * (q % (BM / 2)), kk = q / (BM / 2);
-              double2 v = reinterpret_cast<const double2*>(rs)[(kk * BM + mm) / 2];
-              if (k0 + kk >= a.ks) v = make_double2(0.0, 0.0);
-              accA[e] = (t == 0) ? make_double2(c * v.x, c * v.y)
-                                 : make_double2(fma(c, v.x, accA[e].x), fma(c, v.y, accA[e].y));
-            }
-          }
-        }
-        if (!ks.dirB && t < it.p.nb) {
-          const Term tm = t == 0 ? it.tb : a.terms[it.p.b0 + t];
-          const double c = tm.coef;
-          const int shift = (tm.row * a.ks) & 1;
-          const double* rb = rs + TRAW_A;
-#pragma unroll
-          for (int e = 0; e < FPAIRS; ++e) {
-            const int q = ft + e * NFOLD;
-            if (q < BN * BK / 2) {
-              const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
-              double v0 = rb[nn * TB_K + kk + shift], v1 = rb[nn * TB_K + kk + 1 + shift];
-              if (k0 + kk >= a.ks) v0 = 0.0;
-              if (k0 + kk + 1 >= a.ks) v1 = 0.0;
-              accB[e] = (t == 0) ? make_double2(c * v0, c * v1)
-                                 : make_double2(fma(c, v0, accB[e].x), fma(c, v1, accB[e].y));
-            }
-          }
-        }
+        const bool hasA = !ks.dirA && t < it.p.na, hasB = !ks.dirB && t < it.p.nb;
+        if (kvalid >= BK)
+          fold_slot<false>(rs, meta[slot], hasA, hasB, t == 0, accA, accB, ft, kvalid);
+        else
+          fold_slot<true>(rs, meta[slot], hasA, hasB, t == 0, accA, accB, ft, kvalid);
         __syncwarp();
         if (lane == 0) mbar_arrive(rempty0 + 8 * slot);
       }
@@ -607,12 +644,9 @@ __device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw,
       }
       if (!ks.dirB) {
 #pragma unroll
-        for (int e = 0; e < FPAIRS; ++e) {
+        for (int e = 0; e < FELEMS; ++e) {
           const int q = ft + e * NFOLD;
-          if (q < BN * BK / 2) {
-            const int kk = 2 * (q % (BK / 2)), nn = q / (BK / 2);
-            *reinterpret_cast<double2*>(opB + nn * LDB_S + kk) = accB[e];
-          }
+          if (q < BN * BK) opB[(q / BK) * LDB_S + q % BK] = accB[e];
         }
       }
     }
@@ -763,8 +797,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
   extern __shared__ __align__(128) double smem[];
   double* stages = smem;                                  // [NSTAGE][STAGE_SZ]
   double* raw = stages + (size_t)NSTAGE * STAGE_SZ;       // [NRAW][RAW_SZ] or [NRAW_TMA][TRAW_SZ]
-  unsigned long long* bars =
-      reinterpret_cast<unsigned long long*>(raw + (TMA ? (size_t)NRAW_TMA * TRAW_SZ : (size_t)NRAW * RAW_SZ));
+  SlotMeta* meta = reinterpret_cast<SlotMeta*>(raw + (TMA ? (size_t)NRAW_TMA * TRAW_SZ : (size_t)NRAW * RAW_SZ));
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(meta + (TMA ? NRAW_TMA : 0));
   const unsigned full0 = smem_u32(bars);
   const unsigned empty0 = smem_u32(bars + NSTAGE);
   const unsigned rfull0 = smem_u32(bars + 2 * NSTAGE);
@@ -790,9 +824,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
     if (TMA) {
       if (tid == 0)
-        tma_issuer(a, stages, raw, full0, empty0, rfull0, rempty0, nks);
+        tma_issuer(a, stages, raw, meta, full0, empty0, rfull0, rempty0, nks);
       else if (tid >= 32)
-        tma_folder(a, stages, raw, full0, empty0, rfull0, rempty0, tid - 32, nks);
+        tma_folder(a, stages, raw, meta, full0, empty0, rfull0, rempty0, tid - 32, nks);
     } else {
       producer(a, stages, raw, full0, empty0, tid, nks);
     }
@@ -802,8 +836,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
   }
 }
 
-// S_r / T_r temporaries of the NAIVE pack type: out_r = sum_t coef_t * X_{blk_t}.
-// side 0 uses the A terms of each product, side 1 the B terms.
+// Operand sums in HBM: out_j = sum_t coef_t * X_{blk_t} for the A terms (side 0) or the
+// B terms (side 1) of product plist[j] (j = blockIdx.y).  Used for the NAIVE pack
+// type's S_r / T_r temporaries and for the pre-summed operands of the ABC pack type.
+// Each thread handles two consecutive rows of a column (16-byte loads and stores when
+// the addresses allow).
 struct LincombArgs {
   const double* X;
   long long ldx;
@@ -812,32 +849,50 @@ struct LincombArgs {
   int blk_col_stride;      // cols per block column (ks for A, ns for B)
   double* out;
   long long ldo;
-  long long out_stride;    // per product
+  long long out_stride;    // per output
   const Prod* prods;
   const Term* terms;
+  const int* plist;        // product of each output; nullptr = output j is product j
   int side;
-  int r_begin;
 };
 
 __global__ void fmm_lincomb_kernel(const LincombArgs a) {
-  const int r = a.r_begin + blockIdx.y;
+  const int j = blockIdx.y;
+  const int r = a.plist ? a.plist[j] : j;
   const Prod p = a.prods[r];
   const int t0 = a.side == 0 ? p.a0 : p.b0;
   const int nt = a.side == 0 ? p.na : p.nb;
-  double* out = a.out + (long long)blockIdx.y * a.out_stride;
-  const long long total = (long long)a.rows * a.cols;
+  double* out = a.out + (long long)j * a.out_stride;
+  const int hr = (a.rows + 1) / 2;  // row pairs per column
+  const long long total = (long long)hr * a.cols;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e % a.rows);
-    const long long j = e / a.rows;
-    double v = 0.0;
+    const int i = 2 * (int)(e % hr);
+    const long long c = e / hr;
+    const bool two = i + 1 < a.rows;
+    double v0 = 0.0, v1 = 0.0;
     for (int t = 0; t < nt; ++t) {
       const Term tm = a.terms[t0 + t];
-      const double x = a.X[(long long)tm.row * a.blk_row_stride + i +
-                           ((long long)tm.col * a.blk_col_stride + j) * a.ldx];
-      v = (t == 0) ? tm.coef * x : fma(tm.coef, x, v);
+      const double* x = a.X + (long long)tm.row * a.blk_row_stride + i + ((long long)tm.col * a.blk_col_stride + c) * a.ldx;
+      double x0, x1 = 0.0;
+      if (two && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        const double2 xx = *reinterpret_cast<const double2*>(x);
+        x0 = xx.x;
+        x1 = xx.y;
+      } else {
+        x0 = x[0];
+        if (two) x1 = x[1];
+      }
+      v0 = (t == 0) ? tm.coef * x0 : fma(tm.coef, x0, v0);
+      v1 = (t == 0) ? tm.coef * x1 : fma(tm.coef, x1, v1);
     }
-    out[i + j * a.ldo] = v;
+    double* o = out + i + c * a.ldo;
+    if (two && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+      *reinterpret_cast<double2*>(o) = make_double2(v0, v1);
+    } else {
+      o[0] = v0;
+      if (two) o[1] = v1;
+    }
   }
 }
 

@@ -93,6 +93,10 @@ ORACLE_CASES = [
     (["424"], [1], (300, 256, 200)),
     (["336"], [1], (288, 400, 150)),
     (["222", "232"], [1, 1], (333, 222, 211)),
+    # large enough that the ABC pack type pre-sums operands in HBM (ms*ns >= 2^20, ks >= 256)
+    (["222"], [1], (2056, 2052, 606)),
+    (["333"], [1], (3080, 3090, 800)),
+    (["424"], [1], (4104, 2060, 1034)),
 ]
 
 
