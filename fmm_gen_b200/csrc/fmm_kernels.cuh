@@ -79,8 +79,9 @@ constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_S
                                   (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long);
 constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
 constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
-constexpr int PROD_REGS = 80;
-constexpr int CONS_REGS = 176;
+constexpr int C_PREFETCH_STEPS = 24;  // k steps before a product's end at which its C tiles are prefetched
+constexpr int PROD_REGS = 72;
+constexpr int CONS_REGS = 184;
 static_assert(NPROD * PROD_REGS + NCONS * CONS_REGS <= NTHREADS * LAUNCH_REGS,
               "register split exceeds the launch budget");
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ULL;  // bounded device-side waits give up after 4 s
@@ -429,7 +430,7 @@ __device__ __forceinline__ void fold_unit(const LoadIter& it, const double* raw_
   }
 }
 
-__device__ void producer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0, int pt,
+__device__ __forceinline__ void producer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0, int pt,
                          int nks) {
   LoadIter iss, con;
   load_iter_start(a, iss, nks);
@@ -519,7 +520,7 @@ __device__ __forceinline__ void kiter_next(const GemmArgs& a, LoadIter& it, int 
   load_terms(a, it);
 }
 
-__device__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, SlotMeta* meta, unsigned full0,
+__device__ __forceinline__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, SlotMeta* meta, unsigned full0,
                            unsigned empty0, unsigned rfull0, unsigned rempty0, int nks) {
   LoadIter it;
   kiter_start(a, it, nks);
@@ -598,7 +599,7 @@ __device__ __forceinline__ void fold_slot(const double* rs, const SlotMeta& m, b
   }
 }
 
-__device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, const SlotMeta* meta,
+__device__ __forceinline__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, const SlotMeta* meta,
                            unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft, int nks) {
   LoadIter it;
   kiter_start(a, it, nks);
@@ -629,6 +630,7 @@ __device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw,
           fold_slot<false>(rs, meta[slot], hasA, hasB, t == 0, accA, accB, ft, kvalid);
         else
           fold_slot<true>(rs, meta[slot], hasA, hasB, t == 0, accA, accB, ft, kvalid);
+        __threadfence_block();  // raw-slot loads complete before the slot can be refilled
         __syncwarp();
         if (lane == 0) mbar_arrive(rempty0 + 8 * slot);
       }
@@ -649,6 +651,9 @@ __device__ void tma_folder(const GemmArgs& a, double* stages, const double* raw,
           if (q < BN * BK) opB[(q / BK) * LDB_S + q % BK] = accB[e];
         }
       }
+      // The stage is written here through the generic proxy and later refilled by TMA
+      // (async proxy): order these stores before any later async-proxy access to it.
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(full0 + 8 * stage);
@@ -701,6 +706,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
           }
     return;
   }
+  // C_l += w * M_r, 8 elements at a time: all loads of a batch are issued before any
+  // store, so a batch costs one memory round trip instead of one per element.
 #pragma unroll 1
   for (int c = 0; c < p.nc; ++c) {
     const Term tm = a.terms[p.c0 + c];
@@ -709,18 +716,46 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int jb = 0; jb < 4; jb += 2) {
+        double cv[2][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
-            const int cc = n0 + wn * 32 + j * 8 + t4 * 2 + q;
-            if (rr < a.ms && cc < a.ns) {
-              double* ptr = Cb + rr + (long long)cc * a.ldc;
-              *ptr = fma(w, acc[i][j][2 * h + q], *ptr);
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
+              const int cc = n0 + wn * 32 + (jb + j) * 8 + t4 * 2 + q;
+              cv[j][2 * h + q] = (rr < a.ms && cc < a.ns) ? Cb[rr + (long long)cc * a.ldc] : 0.0;
             }
-          }
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
+              const int cc = n0 + wn * 32 + (jb + j) * 8 + t4 * 2 + q;
+              if (rr < a.ms && cc < a.ns)
+                Cb[rr + (long long)cc * a.ldc] = fma(w, acc[i][jb + j][2 * h + q], cv[j][2 * h + q]);
+            }
+      }
+  }
+}
+
+// Pull the C tiles an epilogue will update into L2 while the product's last k steps run.
+__device__ __forceinline__ void prefetch_c_tiles(const GemmArgs& a, const Prod& p, int m0, int n0, int ct) {
+  if (a.mode != MODE_ACCUM_C) return;
+  for (int c = 0; c < p.nc; ++c) {
+    const Term tm = a.terms[p.c0 + c];
+    const double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc;
+#pragma unroll
+    for (int e = 0; e < (BN * BM / 16) / NCONS; ++e) {  // 128-byte lines: 16 rows of one column
+      const int l = ct + e * NCONS;
+      const int rr = m0 + (l % (BM / 16)) * 16, cc = n0 + l / (BM / 16);
+      if (rr < a.ms && cc < a.ns)
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Cb + rr + (long long)cc * a.ldc));
+    }
   }
 }
 
@@ -749,7 +784,7 @@ __device__ __forceinline__ void ticket_release(const GemmArgs& a, int tile, int 
   if (ct == 0) st_release(a.tickets + tile, chunk + 1);
 }
 
-__device__ void consumer(const GemmArgs& a, const double* stages, unsigned full0, unsigned empty0, int ct, int nks) {
+__device__ __forceinline__ void consumer(const GemmArgs& a, const double* stages, unsigned full0, unsigned empty0, int ct, int nks) {
   const int warp = ct >> 5, lane = ct & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
@@ -777,7 +812,12 @@ __device__ void consumer(const GemmArgs& a, const double* stages, unsigned full0
         const double* opA = stages + (size_t)stage * STAGE_SZ;
         const double* opB = opA + OPA_SZ;
         mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), a.status);
+        if (s == nks - C_PREFETCH_STEPS) prefetch_c_tiles(a, p, w.m0, w.n0, ct);
         mma_stage(opA, opB, acc, wm, wn, g, t4);
+        // The stage is refilled by TMA as soon as every warp has arrived; the fence
+        // makes this warp's shared-memory fragment loads complete before its arrival
+        // (measured: without it a refill could overwrite fragments still in flight).
+        __threadfence_block();
         __syncwarp();
         if (lane == 0) mbar_arrive(empty0 + 8 * stage);
         ++kc;
