@@ -252,3 +252,21 @@ def test_gpu_full_size_within_error_bound(algs, levels, shape, pack):
     assert (D - ref).abs().max().item() <= algebra.error_bound(algebra.classical_plan(), m, n, k, 1, 1, 1)
     del A, B, C, D, ref, C0
     torch.cuda.empty_cache()
+
+
+def test_gpu_torch_custom_op(oracle_lib):
+    """torch.ops.fmm.gemm / fmm.plain_gemm mutate C in place, stream-ordered."""
+    from fmm_gen_b200 import ops  # noqa: F401  (registers the ops)
+
+    m, n, k = 300, 260, 220
+    A, B, C = inputs(41, m, n, k)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    torch.ops.fmm.gemm(dA, dB, dC, "222-1_232-1", "abc")
+    want = C.copy(order="F")
+    oracle_lib.fmm(tables(algebra.make_plan(["222", "232"], [1, 1])), "abc", A, B, want)
+    assert rel_fro(dC.cpu().numpy(), want) <= RTOL_SMALL
+    dC2 = to_dev(C)
+    torch.ops.fmm.plain_gemm(dA, dB, dC2)
+    want2 = C.copy(order="F")
+    oracle_lib.bl_dgemm(A, B, want2)
+    assert rel_fro(dC2.cpu().numpy(), want2) <= RTOL_SMALL
