@@ -842,6 +842,7 @@ const char* fmm_error_string(int code) {
     case FMM_E_PLAN: return "malformed plan tables";
     case FMM_E_UNSUPPORTED: return "unsupported pack type or option";
     case FMM_E_TIMEOUT: return "device-side wait timed out";
+    case FMM_E_TOO_LARGE: return "problem exceeds the no-allocation scratch limits";
     default: return "unknown error";
   }
 }
@@ -891,3 +892,180 @@ int fmm_profile_num_kinds(void) { return K_NUM; }
 const char* fmm_profile_kind_name(int kind) { return (kind >= 0 && kind < K_NUM) ? kKernelNames[kind] : ""; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------
+// No-allocation entry point.
+//
+// Some callers cannot allocate device memory when they call us: frameworks that own the
+// whole device memory through their own arena or caching allocator and forbid foreign
+// cudaMalloc calls (an allocation behind their back can fail or fragment their pool),
+// and code on latency-critical paths where an allocation (or the synchronisation a
+// cudaFree implies) is not acceptable.  fmm_dgemm_dev_noalloc() serves them: it runs the
+// ABC FMM with the operand sums folded during staging (no pre-summed workspace), and
+// keeps the only scratch the kernel needs -- per-tile tickets, the device status word --
+// and the plan tables in one statically allocated device array.
+// ------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxTiles = 16384;   // tile positions (128 x 128) of one call
+constexpr int kNoAllocMaxProds = 1024;    // products of a plan
+constexpr int kNoAllocMaxTerms = 12288;   // A, B and C terms of a plan
+constexpr size_t kNoAllocTicketsOff = 0;
+constexpr size_t kNoAllocStatusOff = kNoAllocTicketsOff + sizeof(int) * kNoAllocMaxTiles;
+constexpr size_t kNoAllocProdsOff = kNoAllocStatusOff + 256;
+constexpr size_t kNoAllocTermsOff = kNoAllocProdsOff + sizeof(fmm::Prod) * (kNoAllocMaxProds + 1);
+constexpr size_t kNoAllocBytes = kNoAllocTermsOff + sizeof(fmm::Term) * (kNoAllocMaxTerms + 3);
+
+}  // namespace
+
+// Every GPU that loads this library holds this array (about 384 KB) until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices];  // device address of g_noalloc_scratch, per device
+bool g_noalloc_ready[kMaxDevices];
+
+// Once per device, with that device current: resolve the array's device address (in host
+// code the symbol is only a host-side stand-in) and configure the kernels.  Nothing here
+// allocates device memory.
+int noalloc_setup(int dev) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ready[dev]) return FMM_OK;
+  void* p = nullptr;
+  FMM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  if (p == nullptr) return FMM_E_CUDA;
+  FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)fmm::smem_bytes(false)));
+  FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)fmm::smem_bytes(true)));
+  int nsm = 0;
+  FMM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  {
+    std::lock_guard<std::mutex> lk2(g_attr_mu);
+    if (sm_count[dev] == 0) sm_count[dev] = nsm;
+    if (!g_encode_tiled) {
+      cudaDriverEntryPointQueryResult q;
+      void* fn = nullptr;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess)
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+  }
+  g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  g_noalloc_ready[dev] = true;
+  return FMM_OK;
+}
+
+// One launch of fmm_gemm_kernel in MODE_ACCUM_C with caller-provided tables, tickets and
+// status word (nothing allocated).
+int noalloc_launch(const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
+                   const double* A, long long lda, const double* B, long long ldb, double* C, long long ldc,
+                   int ms, int ns, int ks, int* tickets, unsigned* status, int nsm, cudaStream_t st) {
+  if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
+  fmm::GemmArgs a{};
+  a.A = A;
+  a.lda = lda;
+  a.B = B;
+  a.ldb = ldb;
+  a.Aw = A;
+  a.ldaw = lda;
+  a.Bw = B;
+  a.ldbw = ldb;
+  a.C = C;
+  a.ldc = ldc;
+  a.ms = ms;
+  a.ns = ns;
+  a.ks = ks;
+  a.prods = prods;
+  a.terms = terms;
+  a.nprod = nprod;
+  a.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
+  a.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
+  a.mode = fmm::MODE_ACCUM_C;
+  a.status = status;
+  const int ntiles = a.tiles_m * a.tiles_n;
+  a.chunks = choose_chunks(ntiles, nprod, nsm);
+  a.tickets = tickets;
+  if (a.chunks > 1) FMM_CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int) * ntiles, st));
+  const long long units = (long long)ntiles * a.chunks;
+  const unsigned grid = (unsigned)(units < nsm ? units : nsm);
+  const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * ks,
+                  bn = (long long)grid_dims[2] * ns;
+  const bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
+                   make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
+                   make_tensor_map(&a.tmB2, B, ak, bn, ldb, fmm::TB_K, fmm::BN);
+  a.tmAw = a.tmA;
+  a.tmBw = a.tmB;
+  a.tmBw2 = a.tmB2;
+  if (tma)
+    fmm::fmm_gemm_kernel<true><<<grid, fmm::NTHREADS, fmm::smem_bytes(true), st>>>(a);
+  else
+    fmm::fmm_gemm_kernel<false><<<grid, fmm::NTHREADS, fmm::smem_bytes(false), st>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int fmm_dgemm_dev_noalloc(const fmm_plan* plan, int m, int n, int k, const double* A, long lda,
+                                     const double* B, long ldb, double* C, long ldc, void* stream, int sync) {
+  if (!plan) return FMM_E_NOPLAN;
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK) return rc;
+  if (m == 0 || n == 0 || k == 0) return FMM_OK;
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // size limits of the static scratch
+  const int pm = plan->dims[0] * kMR, pk = plan->dims[1], pn = plan->dims[2] * kNR;
+  const int md = m - m % pm, kd = k - k % pk, nd = n - n % pn;
+  const int ms = md / plan->dims[0], ks = kd / plan->dims[1], ns = nd / plan->dims[2];
+  const long long tiles_fmm = (long long)((ms + fmm::BM - 1) / fmm::BM) * ((ns + fmm::BN - 1) / fmm::BN);
+  if ((int)plan->prods.size() > kNoAllocMaxProds || (int)plan->terms.size() > kNoAllocMaxTerms ||
+      tiles_fmm > kNoAllocMaxTiles)
+    return FMM_E_TOO_LARGE;
+  rc = noalloc_setup(dev);
+  if (rc != FMM_OK) return rc;
+  unsigned char* base = g_noalloc_ptr[dev];
+  int* tickets = reinterpret_cast<int*>(base + kNoAllocTicketsOff);
+  unsigned* status = reinterpret_cast<unsigned*>(base + kNoAllocStatusOff);
+  fmm::Prod* prods = reinterpret_cast<fmm::Prod*>(base + kNoAllocProdsOff);
+  fmm::Term* terms = reinterpret_cast<fmm::Term*>(base + kNoAllocTermsOff);
+  // plan tables, then the classical product (index kNoAllocMaxProds, terms after the plan's)
+  const fmm::Prod classic{kNoAllocMaxTerms, 1, kNoAllocMaxTerms + 1, 1, kNoAllocMaxTerms + 2, 1};
+  const fmm::Term one{0, 0, 1.0, 0, 0};
+  const fmm::Term classic_terms[3] = {one, one, one};
+  FMM_CUDA_TRY(cudaMemcpyAsync(prods, plan->prods.data(), sizeof(fmm::Prod) * plan->prods.size(),
+                               cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyAsync(terms, plan->terms.data(), sizeof(fmm::Term) * plan->terms.size(),
+                               cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyAsync(prods + kNoAllocMaxProds, &classic, sizeof(classic), cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemcpyAsync(terms + kNoAllocMaxTerms, classic_terms, sizeof(classic_terms),
+                               cudaMemcpyHostToDevice, st));
+  FMM_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
+  const int nsm = sm_count[dev] > 0 ? sm_count[dev] : 148;
+  rc = noalloc_launch(prods, terms, plan->dims, plan->rank, A, lda, B, ldb, C, ldc, ms, ns, ks, tickets, status, nsm,
+                      st);
+  // fringe GEMMs (same regions and order as the reference's dynamic peeling)
+  const int mr = m - md, kr = k - kd, nr = n - nd;
+  const fmm::Prod* cp = prods + kNoAllocMaxProds;
+  if (rc == FMM_OK && kr > 0 && md > 0 && nd > 0)
+    rc = noalloc_launch(cp, terms, kUnitGrid, 1, A + (long long)kd * lda, lda, B + kd, ldb, C, ldc, md, nd, kr,
+                        tickets, status, nsm, st);
+  if (rc == FMM_OK && nr > 0)
+    rc = noalloc_launch(cp, terms, kUnitGrid, 1, A, lda, B + (long long)nd * ldb, ldb, C + (long long)nd * ldc, ldc, m,
+                        nr, k, tickets, status, nsm, st);
+  if (rc == FMM_OK && mr > 0 && nd > 0)
+    rc = noalloc_launch(cp, terms, kUnitGrid, 1, A + md, lda, B, ldb, C + md, ldc, mr, nd, k, tickets, status, nsm,
+                        st);
+  if (rc == FMM_OK && sync) {
+    unsigned v = 0;
+    FMM_CUDA_TRY(cudaMemcpyAsync(&v, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (v) rc = FMM_E_TIMEOUT;
+  }
+  return rc;
+}

@@ -35,6 +35,7 @@ extern "C" {
 #define FMM_E_PLAN (-5)         /* malformed plan tables */
 #define FMM_E_UNSUPPORTED (-6)  /* pack type or option not supported */
 #define FMM_E_TIMEOUT (-7)      /* a bounded device-side wait gave up */
+#define FMM_E_TOO_LARGE (-8)    /* beyond the fixed limits of fmm_dgemm_dev_noalloc */
 
 #define FMM_PACK_ABC 0    /* sums fused into operand staging, products scattered into C */
 #define FMM_PACK_AB 1     /* sums fused into staging, each product to a workspace M_r, then scatter */
@@ -100,6 +101,24 @@ int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, con
  * FMM_OK otherwise.  Synchronises with the device; clear != 0 resets the word.  The
  * synchronous host entry points check it themselves. */
 int fmm_device_status(int clear);
+
+/* FMM C += A*B (pack type ABC) that allocates no memory -- no counterpart in the
+ * reference.  For callers that cannot allocate device memory at call time: frameworks
+ * that own all device memory through their own arena or caching allocator, and
+ * latency-critical paths where an allocation is not acceptable.  Operand sums are
+ * folded while staging (no workspace); the only scratch -- per-tile tickets, a status
+ * word and the plan's tables -- lives in one statically allocated device array (about
+ * 384 KB, held by every GPU that loads the library until the process exits).
+ *   Limits: plan with <= 1024 products and <= 12288 terms; <= 16384 tiles of 128 x 128
+ *   in a product (ms x ns); beyond them it returns FMM_E_TOO_LARGE without running.
+ *   The first call on a device resolves the array's address (cudaGetSymbolAddress) and
+ *   configures the kernels; make that first call before any stream capture.
+ *   Every call shares the array: calls that overlap on the GPU (other streams, other
+ *   host threads) race; serialise them on one stream.
+ *   sync != 0: synchronise the stream and report a device-side wait timeout
+ *   (FMM_E_TIMEOUT); sync == 0: stream-ordered, launch errors only. */
+int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const double *A, long lda, const double *B,
+                          long ldb, double *C, long ldc, void *stream, int sync);
 
 /* Number of kernels the library launched since load (all entry points, all streams). */
 long long fmm_kernel_launch_count(void);
