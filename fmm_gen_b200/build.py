@@ -28,7 +28,7 @@ def nvcc() -> str:
 
 
 SOURCES = ["fmm_capi.cu"]
-HEADERS = ["fmm_kernels.cuh", os.path.join("..", "..", "include", "fmm_b200.h")]
+HEADERS = ["fmm_kernels.cuh", "fmm_split_bf16.cuh", os.path.join("..", "..", "include", "fmm_b200.h")]
 
 
 def _stale(target: str, deps) -> bool:

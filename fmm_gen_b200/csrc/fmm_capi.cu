@@ -22,6 +22,7 @@
 
 #include "../../include/fmm_b200.h"
 #include "fmm_kernels.cuh"
+#include "fmm_split_bf16.cuh"
 
 namespace {
 
@@ -34,9 +35,18 @@ thread_local int t_last_error = FMM_OK;
 
 // Optional per-kernel timing: when enabled, every launch is bracketed by CUDA events on
 // its own stream; fmm_profile_end() sums the durations per kernel kind.
-enum KernelKind { K_GEMM_FMM = 0, K_GEMM_CLASSICAL = 1, K_LINCOMB = 2, K_SCATTER = 3, K_NUM = 4 };
+enum KernelKind {
+  K_GEMM_FMM = 0,
+  K_GEMM_CLASSICAL = 1,
+  K_LINCOMB = 2,
+  K_SCATTER = 3,
+  K_SPLIT_OPERANDS = 4,
+  K_GEMM_SPLIT = 5,
+  K_NUM = 6
+};
 const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
-                                         "fmm_lincomb_kernel", "fmm_scatter_kernel"};
+                                         "fmm_lincomb_kernel", "fmm_scatter_kernel",
+                                         "fmm_split_operands_kernel", "fmm_split_gemm_kernel"};
 struct ProfRec {
   int kind;
   cudaEvent_t e0, e1;
@@ -1068,4 +1078,171 @@ extern "C" int fmm_dgemm_dev_noalloc(const fmm_plan* plan, int m, int n, int k, 
     if (v) rc = FMM_E_TIMEOUT;
   }
   return rc;
+}
+
+// ---------------------------------------------------------------------------------------
+// Split-BF16 FMM (tcgen05 tensor cores): FP32 A and B, FP64 C.  Same partition, product
+// order and fringe peeling as the FP64 path; every GEMM (FMM core and fringe strips) runs
+// as bf16 plane products with FP64 accumulation across 64-deep k chunks.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+bool split_configured[kMaxDevices];
+
+int split_configure(int* dev_out) {
+  int rc = configure_kernel(dev_out);
+  if (rc != FMM_OK) return rc;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (!split_configured[*dev_out]) {
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmms::fmm_split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmms::SMEM_BYTES));
+    split_configured[*dev_out] = true;
+  }
+  return g_encode_tiled ? FMM_OK : FMM_E_UNSUPPORTED;
+}
+
+// bf16 planes (rows x kpad, row-major, pitch kpad) as a tensor map with box 64 x 128 and
+// the 128-byte swizzle the UMMA descriptors expect.
+bool make_plane_map(CUtensorMap* map, const __nv_bfloat16* base, long long rows, long long kpad) {
+  if (rows <= 0 || rows >= (1LL << 32) || kpad % fmms::KPAD != 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kpad * sizeof(__nv_bfloat16)};
+  cuuint32_t box[2] = {(cuuint32_t)fmms::BK, (cuuint32_t)fmms::BM};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode_tiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims,
+                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// One split-BF16 launch pair over sub-blocks ms x ks x ns of a plan (R products):
+// operand planes into a stream-ordered workspace, then the persistent tcgen05 GEMM.
+int split_core(const DevTables& d, int R, const float* A, long long lda, const float* B, long long ldb, double* C,
+               long long ldc, int ms, int ns, int ks, cudaStream_t st) {
+  if (ms <= 0 || ns <= 0 || ks <= 0) return FMM_OK;
+  int dev = 0;
+  int rc = split_configure(&dev);
+  if (rc != FMM_OK) return rc;
+  static_assert(fmms::BM == fmms::BN, "one box shape for both plane maps");
+  const long long kpad = ((long long)ks + fmms::KPAD - 1) / fmms::KPAD * fmms::KPAD;
+  const long long rows_a = 3LL * R * ms, rows_b = 3LL * R * ns;
+  const int tiles_m = (ms + fmms::BM - 1) / fmms::BM, tiles_n = (ns + fmms::BN - 1) / fmms::BN;
+  const long long ntiles = (long long)tiles_m * tiles_n;
+  if (ntiles * R > INT32_MAX || (ms + fmms::SPLIT_ROWS - 1) / fmms::SPLIT_ROWS > 65535 ||
+      (ns + fmms::SPLIT_ROWS - 1) / fmms::SPLIT_ROWS > 65535 || kpad / fmms::SPLIT_K > 65535)
+    return FMM_E_UNSUPPORTED;
+  const size_t bytes_a = sizeof(__nv_bfloat16) * (size_t)(rows_a * kpad);
+  const size_t bytes_b = sizeof(__nv_bfloat16) * (size_t)(rows_b * kpad);
+  const size_t bytes_t = R > 1 ? sizeof(int) * (size_t)ntiles : 0;
+  char* ws = nullptr;
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes_a + bytes_b + bytes_t + 16, st));
+  __nv_bfloat16* PA = reinterpret_cast<__nv_bfloat16*>(ws);
+  __nv_bfloat16* PB = reinterpret_cast<__nv_bfloat16*>(ws + bytes_a);
+  int* tickets = R > 1 ? reinterpret_cast<int*>(ws + bytes_a + bytes_b) : nullptr;
+  if (tickets) rc = cuda_status(cudaMemsetAsync(tickets, 0, bytes_t, st));
+
+  fmms::SplitArgs sa{};
+  sa.X = A;
+  sa.ldx = lda;
+  sa.rows = ms;
+  sa.ks = ks;
+  sa.kpad = (int)kpad;
+  sa.blk_row_stride = ms;
+  sa.blk_col_stride = ks;
+  sa.out = PA;
+  sa.prods = d.prods;
+  sa.terms = d.terms;
+  sa.side = 0;
+  fmms::SplitArgs sb = sa;
+  sb.X = B;
+  sb.ldx = ldb;
+  sb.rows = ns;
+  sb.blk_row_stride = ks;
+  sb.blk_col_stride = ns;
+  sb.out = PB;
+  sb.side = 1;
+  if (rc == FMM_OK) {
+    ProfScope pf(K_SPLIT_OPERANDS, st);
+    const dim3 blk(32, 8);
+    const unsigned kt = (unsigned)(kpad / fmms::SPLIT_K);
+    fmms::fmm_split_operands_kernel<<<dim3((unsigned)R, kt, (unsigned)((ms + fmms::SPLIT_ROWS - 1) / fmms::SPLIT_ROWS)),
+                                      blk, 0, st>>>(sa);
+    fmms::fmm_split_operands_kernel<<<dim3((unsigned)R, kt, (unsigned)((ns + fmms::SPLIT_ROWS - 1) / fmms::SPLIT_ROWS)),
+                                      blk, 0, st>>>(sb);
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    rc = cuda_status(cudaGetLastError());
+  }
+  fmms::SplitGemmArgs g{};
+  if (rc == FMM_OK && (!make_plane_map(&g.tmA, PA, rows_a, kpad) || !make_plane_map(&g.tmB, PB, rows_b, kpad)))
+    rc = FMM_E_UNSUPPORTED;
+  if (rc == FMM_OK) {
+    g.C = C;
+    g.ldc = ldc;
+    g.ms = ms;
+    g.ns = ns;
+    g.kpad = (int)kpad;
+    g.prods = d.prods;
+    g.terms = d.terms;
+    g.nprod = R;
+    g.tiles_m = tiles_m;
+    g.tiles_n = tiles_n;
+    g.tickets = tickets;
+    g.status = dev_status[dev];
+    const long long units = ntiles * R;
+    const unsigned grid = (unsigned)(units < sm_count[dev] ? units : sm_count[dev]);
+    {
+      ProfScope pf(K_GEMM_SPLIT, st);
+      fmms::fmm_split_gemm_kernel<<<grid, fmms::NTHREADS, fmms::SMEM_BYTES, st>>>(g);
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    rc = cuda_status(cudaGetLastError());
+  }
+  cudaError_t fe = cudaFreeAsync(ws, st);
+  if (rc == FMM_OK) rc = cuda_status(fe);
+  return rc;
+}
+
+int split_plain(int m, int n, int k, const float* A, long long lda, const float* B, long long ldb, double* C,
+                long long ldc, cudaStream_t st) {
+  if (m <= 0 || n <= 0 || k <= 0) return FMM_OK;
+  DevTables* d = nullptr;
+  int rc = device_tables(classical_plan(), &d);
+  if (rc != FMM_OK) return rc;
+  return split_core(*d, 1, A, lda, B, ldb, C, ldc, m, n, k, st);
+}
+
+int run_split(const fmm_plan* plan, int m, int n, int k, const float* A, long long lda, const float* B,
+              long long ldb, double* C, long long ldc, cudaStream_t st) {
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK || m == 0 || n == 0 || k == 0) return rc;
+  if (!plan) return split_plain(m, n, k, A, lda, B, ldb, C, ldc, st);
+  const int pm = plan->dims[0] * kMR, pk = plan->dims[1], pn = plan->dims[2] * kNR;
+  const int mr = m % pm, kr = k % pk, nr = n % pn;
+  const int md = m - mr, kd = k - kr, nd = n - nr;
+  if (md > 0 && nd > 0 && kd > 0) {
+    DevTables* d = nullptr;
+    rc = device_tables(plan, &d);
+    if (rc != FMM_OK) return rc;
+    rc = split_core(*d, plan->rank, A, lda, B, ldb, C, ldc, md / plan->dims[0], nd / plan->dims[2],
+                    kd / plan->dims[1], st);
+    if (rc != FMM_OK) return rc;
+  }
+  // fringe strips: the same regions, in the same order, as the FP64 path's peeling
+  if (kr > 0 && md > 0 && nd > 0) {
+    rc = split_plain(md, nd, kr, A + (long long)kd * lda, lda, B + kd, ldb, C, ldc, st);
+    if (rc != FMM_OK) return rc;
+  }
+  if (nr > 0) {
+    rc = split_plain(m, nr, k, A, lda, B + (long long)nd * ldb, ldb, C + (long long)nd * ldc, ldc, st);
+    if (rc != FMM_OK) return rc;
+  }
+  if (mr > 0 && nd > 0) rc = split_plain(mr, nd, k, A + md, lda, B, ldb, C + md, ldc, st);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int fmm_split_gemm_dev(const fmm_plan* plan, int m, int n, int k, const float* A, long lda,
+                                  const float* B, long ldb, double* C, long ldc, void* stream) {
+  return run_split(plan, m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
 }

@@ -84,6 +84,9 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_dgemm_host.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int,
                                    c_void_p, c_int]
     lib.fmm_dgemm_host.restype = c_int
+    lib.fmm_split_gemm_dev.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_long, c_void_p, c_long, c_void_p,
+                                       c_long, c_void_p]
+    lib.fmm_split_gemm_dev.restype = c_int
     for name in ("bl_dgemm", "bl_dgemm_strassen_abc", "bl_dgemm_strassen_ab", "bl_dgemm_strassen_naive"):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]
@@ -181,12 +184,13 @@ def _ld(t, rows: int) -> int:
     return max(t.stride(1), rows, 1) if t.shape[1] > 1 else max(rows, 1)
 
 
-def _check_operands(A, B, C):
+def _check_operands(A, B, C, ab_dtype=None):
     import torch
 
     for name, t in (("A", A), ("B", B), ("C", C)):
-        if t.dtype != torch.float64:
-            raise FmmError(-1, f"{name} must be float64")
+        want = torch.float64 if (name == "C" or ab_dtype is None) else ab_dtype
+        if t.dtype != want:
+            raise FmmError(-1, f"{name} must be {str(want).replace('torch.', '')}")
         if not t.is_cuda:
             raise FmmError(-1, f"{name} must be a CUDA tensor")
     m, k = A.shape
@@ -218,6 +222,21 @@ def plain_gemm(A, B, C, stream=None) -> None:
     rc = lib.fmm_plain_dgemm_dev(m, n, k, A.data_ptr(), _ld(A, m), B.data_ptr(), _ld(B, k), C.data_ptr(),
                                  _ld(C, m), ctypes.c_void_p(s.cuda_stream))
     _check(rc, "fmm_plain_dgemm_dev")
+
+
+def split_gemm(plan, A, B, C, stream=None) -> None:
+    """C += A @ B on the tensor cores at FP32-level accuracy: float32 A and B, float64 C.
+
+    plan=None runs the classical product; otherwise the FMM plan's products, each as six
+    bf16 plane products with FP64 accumulation across 64-deep k chunks."""
+    import torch
+
+    m, n, k = _check_operands(A, B, C, ab_dtype=torch.float32)
+    lib = load_library()
+    s = stream if stream is not None else torch.cuda.current_stream(C.device)
+    rc = lib.fmm_split_gemm_dev(plan.handle if plan is not None else None, m, n, k, A.data_ptr(), _ld(A, m),
+                                B.data_ptr(), _ld(B, k), C.data_ptr(), _ld(C, m), ctypes.c_void_p(s.cuda_stream))
+    _check(rc, "fmm_split_gemm_dev")
 
 
 # --------------------------------------------------------------------------------

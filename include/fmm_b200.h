@@ -120,6 +120,19 @@ int fmm_device_status(int clear);
 int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const double *A, long lda, const double *B,
                           long ldb, double *C, long ldc, void *stream, int sync);
 
+/* Split-BF16 FMM on the tensor cores -- no counterpart in the reference (FP64 only).
+ * C += A*B with FP32 A (m x k), B (k x n) and FP64 C, column-major device pointers,
+ * enqueued on `stream`.  Same partition, product order and fringe peeling as
+ * fmm_dgemm_dev (plan == NULL: classical).  Each product's operand sums are formed in
+ * FP64 and split into three bf16 planes; the product is six bf16 plane products
+ * accumulated in FP32 over 64-deep k chunks and in FP64 across chunks; W[l,r] * M_r is
+ * added to C in FP64.  Relative Frobenius error against the FP64 product of the same
+ * FP32 inputs: about 1e-7 (classical) and a few 1e-7 for two Strassen levels.
+ * Workspace: 6 R (ms + ns) kpad bytes from the stream-ordered allocator
+ * (kpad = ks rounded up to 64). */
+int fmm_split_gemm_dev(const fmm_plan *plan, int m, int n, int k, const float *A, long lda, const float *B,
+                       long ldb, double *C, long ldc, void *stream);
+
 /* Number of kernels the library launched since load (all entry points, all streams). */
 long long fmm_kernel_launch_count(void);
 
