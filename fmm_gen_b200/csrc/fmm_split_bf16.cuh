@@ -9,11 +9,12 @@
 //      of 64, zero padded).  Likewise T_r = sum_j V[j,r] B_j.
 //   2. fmm_split_gemm_kernel: M_r = S_r T_r as six plane products
 //      hi*hi + hi*mid + mid*hi + mid*mid + hi*lo + lo*hi (the dropped ones are ~2^-24
-//      relative), tcgen05.mma kind::f16 into an FP32 accumulator in tensor memory, the
-//      small plane products first so that the accumulator's own rounding acts at the
-//      magnitude of the hi*hi terms only a few times per chunk.  Every
-//      64-deep k chunk is drained with tcgen05.ld and added into FP64 registers, so FP32
-//      rounding only acts within a chunk; the epilogue adds W[l,r] * M_r into FP64 C.
+//      relative), tcgen05.mma kind::f16 into FP32 accumulators in tensor memory: hi*hi
+//      into one, the five smaller products into another, so that the accumulators' own
+//      rounding never drops the small terms against the large ones.  Every 128-deep k
+//      chunk is drained with tcgen05.ld (the two accumulators added once in FP32) and
+//      added into FP64 registers, so FP32 rounding only acts within a chunk; the epilogue
+//      adds W[l,r] * M_r into FP64 C.
 //
 // Work unit = (128 x 128 tile position, product r); a unit owns its tile position in every
 // C block, and per-tile tickets order the products' C updates (no atomics on C, the result
@@ -37,23 +38,26 @@ using fmm::Term;
 
 constexpr int BM = 128;        // tile rows (m) = tensor-memory lanes
 constexpr int BN = 128;        // tile columns (n) = accumulator columns
-constexpr int BK = 64;         // k per stage and per FP64 drain: 64 bf16 = one 128-byte swizzle row
+constexpr int BK = 64;         // k per stage: 64 bf16 = one 128-byte swizzle row
 constexpr int UK = 16;         // k per tcgen05.mma (kind::f16)
 constexpr int NPLANE = 3;
 constexpr int NPAIR = 6;
 constexpr int NSTG = 2;
 constexpr int TILE_BYTES = BM * BK * 2;                  // 16 KB: one plane tile
 constexpr int STAGE_BYTES = 2 * NPLANE * TILE_BYTES;     // 96 KB: three A planes, three B planes
-constexpr int NACC = 4;                                  // accumulators in tensor memory: the MMAs run
+constexpr int NACC = 2;                                  // chunk buffers in tensor memory: the MMAs run
                                                          // up to NACC chunks ahead of the drain
-constexpr int TMEM_COLS = NACC * BN;                     // 512 columns (all of tensor memory)
+constexpr int ACC_COLS = 2 * BN;                         // a chunk buffer: hi*hi accumulator, then the
+                                                         // accumulator of the five smaller plane products
+constexpr int TMEM_COLS = NACC * ACC_COLS;               // 512 columns (all of tensor memory)
 constexpr int NTHREADS = 384;
 constexpr int NEPI = 256;                                // epilogue threads (warps 4..11)
 constexpr int KPAD = 64;                                 // plane row pitch multiple
 constexpr int NBARS = 2 * NSTG + 2 * NACC + 1;
 constexpr size_t SMEM_BYTES = (size_t)NSTG * STAGE_BYTES + 1024 /*alignment slack*/ + 8 * NBARS + 16;
 constexpr int GROUP_M = 8;
-constexpr int C_PREFETCH_CHUNKS = 6;                     // C tiles go to L2 this many chunks before a unit ends
+constexpr int DRAIN_STAGES = 2;                          // stages (of BK) accumulated in FP32 before each FP64 drain
+constexpr int C_PREFETCH_CHUNKS = 4;                     // C tiles go to L2 this many drains before a unit ends
 constexpr int C_BATCH = 16;                              // C elements in flight per thread in the epilogue
 constexpr int LAUNCH_REGS = 65536 / NTHREADS / 8 * 8;    // 168 with one CTA per SM
 constexpr int CTL_REGS = 56;
@@ -115,21 +119,16 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
-// 32 consecutive accumulator columns of this thread's lane (32x32b shape, 32 repeats).
-__device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32]) {
-  unsigned r[32];
+// 16 consecutive accumulator columns of this thread's lane (32x32b shape, 16 repeats);
+// the caller waits (tmem_wait_ld) before using the values.
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
 // Wait for a phase with a time limit only (no early exit on the status word): used at
 // the end of the kernel for copies and MMAs that may still be in flight.
@@ -242,31 +241,38 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(CTL_REGS));
     if (warp == 1 && lane == 0) {  // ---- MMA issuer ----
       constexpr uint32_t idesc = instr_desc_bf16_f32(BM, BN);
-      // plane pairs (A plane, B plane), smallest products first
+      // plane pairs (A plane, B plane); the last, hi*hi, has an accumulator of its own
       constexpr int pa[NPAIR] = {2, 0, 1, 1, 0, 0};
       constexpr int pb[NPAIR] = {0, 2, 1, 0, 1, 0};
-      long long kc = 0;
+      long long kc = 0, ch = 0;
       for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         for (int s = 0; s < nks; ++s, ++kc) {
           const int stg = (int)(kc % NSTG);
-          const int b = (int)(kc % NACC);
+          const int b = (int)(ch % NACC);
+          const bool first = s % DRAIN_STAGES == 0, last = s % DRAIN_STAGES == DRAIN_STAGES - 1 || s == nks - 1;
           fmm::mbar_wait(full0 + 8 * stg, (unsigned)((kc / NSTG) & 1), a.status);
-          fmm::mbar_wait(acce0 + 8 * b, (unsigned)(((kc / NACC) & 1) ^ 1), a.status);
+          if (first) fmm::mbar_wait(acce0 + 8 * b, (unsigned)(((ch / NACC) & 1) ^ 1), a.status);
           tc_fence_after();
           const unsigned base = fmm::smem_u32(smem + (size_t)stg * STAGE_BYTES);
           const uint64_t dbase = smem_desc_sw128(base);
-          const unsigned dt = tmem + (unsigned)(b * BN);
+          const unsigned dt = tmem + (unsigned)(b * ACC_COLS);
 #pragma unroll
           for (int q = 0; q < NPAIR; ++q) {
 #pragma unroll
             for (int kk = 0; kk < BK / UK; ++kk) {
               const uint64_t ad = dbase + (uint64_t)((pa[q] * TILE_BYTES + kk * UK * 2) >> 4);
               const uint64_t bd = dbase + (uint64_t)(((NPLANE + pb[q]) * TILE_BYTES + kk * UK * 2) >> 4);
-              umma_bf16(dt, ad, bd, idesc, (kk | q) != 0);
+              if (q == NPAIR - 1)
+                umma_bf16(dt, ad, bd, idesc, !first || kk != 0);
+              else
+                umma_bf16(dt + BN, ad, bd, idesc, !first || (kk | q) != 0);
             }
           }
           umma_commit(empty0 + 8 * stg);  // stage reusable once these MMAs have read it
-          umma_commit(accf0 + 8 * b);     // chunk ready for the drain
+          if (last) {
+            umma_commit(accf0 + 8 * b);  // chunk ready for the drain
+            ++ch;
+          }
         }
       }
       umma_commit(done_bar);
@@ -279,26 +285,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
     const int quarter = warp & 3, half = (warp - 4) >> 2;
     const int row = quarter * 32 + lane;
     const bool ordered = a.nprod > 1;
-    long long kc = 0;
+    long long ch = 0;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
       const SUnit w = s_decode(a, u);
       double acc[64];
 #pragma unroll
       for (int i = 0; i < 64; ++i) acc[i] = 0.0;
       const Prod p = a.prods[w.r];
-      for (int s = 0; s < nks; ++s, ++kc) {
-        if (s == (nks > C_PREFETCH_CHUNKS ? nks - C_PREFETCH_CHUNKS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, et);
-        const int b = (int)(kc % NACC);
-        fmm::mbar_wait(accf0 + 8 * b, (unsigned)((kc / NACC) & 1), a.status);
+      const int nch = (nks + DRAIN_STAGES - 1) / DRAIN_STAGES;
+      for (int c = 0; c < nch; ++c, ++ch) {
+        if (c == (nch > C_PREFETCH_CHUNKS ? nch - C_PREFETCH_CHUNKS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, et);
+        const int b = (int)(ch % NACC);
+        fmm::mbar_wait(accf0 + 8 * b, (unsigned)((ch / NACC) & 1), a.status);
         tc_fence_after();
-        const unsigned taddr = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)(b * BN + half * 64);
-        float v[32];
-        tmem_ld32(taddr, v);
+        const unsigned taddr = tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)(b * ACC_COLS + half * 64);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) acc[i] += (double)v[i];
-        tmem_ld32(taddr + 32, v);
+        for (int h = 0; h < 4; ++h) {
+          unsigned v[16], e[16];
+          tmem_ld16(taddr + 16 * h, v);
+          tmem_ld16(taddr + BN + 16 * h, e);
+          tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; ++i) acc[32 + i] += (double)v[i];
+          for (int i = 0; i < 16; ++i) acc[16 * h + i] += (double)(__uint_as_float(v[i]) + __uint_as_float(e[i]));
+        }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) fmm::mbar_arrive(acce0 + 8 * b);

@@ -228,7 +228,7 @@ def split_gemm(plan, A, B, C, stream=None) -> None:
     """C += A @ B on the tensor cores at FP32-level accuracy: float32 A and B, float64 C.
 
     plan=None runs the classical product; otherwise the FMM plan's products, each as six
-    bf16 plane products with FP64 accumulation across 64-deep k chunks."""
+    bf16 plane products with FP64 accumulation across 128-deep k chunks."""
     import torch
 
     m, n, k = _check_operands(A, B, C, ab_dtype=torch.float32)
