@@ -12,6 +12,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -42,11 +43,14 @@ enum KernelKind {
   K_SCATTER = 3,
   K_SPLIT_OPERANDS = 4,
   K_GEMM_SPLIT = 5,
-  K_NUM = 6
+  K_GEMM_BATCH = 6,
+  K_LINCOMB_BATCH = 7,
+  K_NUM = 8
 };
 const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
                                          "fmm_lincomb_kernel", "fmm_scatter_kernel",
-                                         "fmm_split_operands_kernel", "fmm_split_gemm_kernel"};
+                                         "fmm_split_operands_kernel", "fmm_split_gemm_kernel",
+                                         "fmm_gemm_batch_kernel", "fmm_lincomb_batch_kernel"};
 struct ProfRec {
   int kind;
   cudaEvent_t e0, e1;
@@ -1246,3 +1250,372 @@ extern "C" int fmm_split_gemm_dev(const fmm_plan* plan, int m, int n, int k, con
                                   const float* B, long ldb, double* C, long ldc, void* stream) {
   return run_split(plan, m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
 }
+
+// ---------------------------------------------------------------------------------------
+// Batches: many independent FP64 problems, each with its own plan (or classical), in one
+// persistent launch.  The reference runs one generated entry point per call
+// (meta/abc_gen_mix.py:448-472); a batch is the GPU form of calling it for many shapes.
+// ---------------------------------------------------------------------------------------
+struct fmm_batch {
+  struct Job {
+    int prob;                      // problem index
+    const fmm_plan* plan;          // tables to run (the classical plan for strips)
+    int grid[3];                   // plan dims (1,1,1 for classical)
+    int ms, ns, ks;                // sub-block sizes
+    int a_r, a_c, b_r, b_c, c_r, c_c;  // operand offsets (row, column) inside the problem
+    bool presum;
+    int nA, nB;                    // pre-summed operand slots
+    size_t ws_off;                 // byte offset of S (then T) in the workspace
+    long long ldT;
+    int chunks, tiles_m, tiles_n, units;
+    size_t ticket_off;             // int offset into the ticket array
+    double cost;                   // estimated k steps per unit (scheduling order)
+  };
+  int count = 0;
+  int dev = 0;
+  std::vector<int> m, n, k;
+  std::vector<const fmm_plan*> plans;
+  std::vector<Job> jobs[2];        // phase 0: FMM cores and disjoint strips; phase 1: k strips
+  std::vector<int> unit_start[2];
+  int max_slots = 0;
+  int n_lincomb = 0;
+  size_t n_tickets = 0, ws_bytes = 0;
+  fmm::GemmArgs* d_jobs[2] = {nullptr, nullptr};
+  int* d_start[2] = {nullptr, nullptr};
+  fmm::GemmArgs* h_jobs[2] = {nullptr, nullptr};  // pinned staging of the job tables
+  fmm::LincombTask* d_lc = nullptr;
+  fmm::LincombTask* h_lc = nullptr;
+  int* d_tickets = nullptr;
+  char* d_ws = nullptr;
+  cudaEvent_t staged = nullptr;    // the staging buffers' last copies are done
+};
+
+namespace {
+
+bool batch_configured[kMaxDevices];
+
+int batch_configure(int* dev) {
+  int rc = configure_kernel(dev);
+  if (rc != FMM_OK) return rc;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  if (!batch_configured[*dev]) {
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::smem_bytes(true)));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::smem_bytes(false)));
+    batch_configured[*dev] = true;
+  }
+  return FMM_OK;
+}
+
+// Products per unit: units of about the work of a 128 x 128 x 4096 classical tile, so the
+// persistent grid balances across problems of very different sizes.
+int batch_chunks(int nprod, int ks) {
+  const long long ksteps = (long long)nprod * ((ks + fmm::BK - 1) / fmm::BK);
+  long long c = (ksteps + 511) / 512;
+  if (c < 1) c = 1;
+  if (c > nprod) c = nprod;
+  return (int)c;
+}
+
+void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int ms, int ns, int ks, int a_r, int a_c,
+                   int b_r, int b_c, int c_r, int c_c) {
+  if (ms <= 0 || ns <= 0 || ks <= 0) return;
+  fmm_batch::Job j{};
+  j.prob = prob;
+  j.plan = plan;
+  std::memcpy(j.grid, plan->dims, sizeof(j.grid));
+  j.ms = ms;
+  j.ns = ns;
+  j.ks = ks;
+  j.a_r = a_r;
+  j.a_c = a_c;
+  j.b_r = b_r;
+  j.b_c = b_c;
+  j.c_r = c_r;
+  j.c_c = c_c;
+  j.presum = plan->rank > 1 && use_presum(plan, ms, ns, ks);
+  if (j.presum) {
+    j.nA = (int)plan->plistA.size();
+    j.nB = (int)plan->plistB.size();
+    j.ldT = ks + (ks & 1);
+    j.ws_off = b->ws_bytes;
+    b->ws_bytes += sizeof(double) * ((size_t)ms * ks * j.nA + (size_t)j.ldT * ns * j.nB);
+    b->ws_bytes = (b->ws_bytes + 255) & ~(size_t)255;
+    b->max_slots = std::max(b->max_slots, std::max(j.nA, j.nB));
+    b->n_lincomb += (j.nA > 0) + (j.nB > 0);
+  }
+  j.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
+  j.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
+  j.chunks = batch_chunks(plan->rank, ks);
+  j.units = j.tiles_m * j.tiles_n * j.chunks;
+  j.ticket_off = b->n_tickets;
+  if (j.chunks > 1) b->n_tickets += (size_t)j.tiles_m * j.tiles_n;
+  j.cost = (double)plan->rank / j.chunks * ((ks + fmm::BK - 1) / fmm::BK);
+  b->jobs[phase].push_back(j);
+}
+
+void batch_free(fmm_batch* b) {
+  for (int ph = 0; ph < 2; ++ph) {
+    if (b->d_jobs[ph]) cudaFree(b->d_jobs[ph]);
+    if (b->d_start[ph]) cudaFree(b->d_start[ph]);
+    if (b->h_jobs[ph]) cudaFreeHost(b->h_jobs[ph]);
+  }
+  if (b->d_lc) cudaFree(b->d_lc);
+  if (b->h_lc) cudaFreeHost(b->h_lc);
+  if (b->d_tickets) cudaFree(b->d_tickets);
+  if (b->d_ws) cudaFree(b->d_ws);
+  if (b->staged) cudaEventDestroy(b->staged);
+  delete b;
+}
+
+int batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
+  if (!out || count <= 0 || !m || !n || !k) return FMM_E_INVALID;
+  for (int i = 0; i < count; ++i)
+    if (m[i] < 0 || n[i] < 0 || k[i] < 0) return FMM_E_INVALID;
+  int dev = 0;
+  int rc = batch_configure(&dev);
+  if (rc != FMM_OK) return rc;
+  fmm_batch* b = new (std::nothrow) fmm_batch();
+  if (!b) return FMM_E_NOMEM;
+  b->count = count;
+  b->dev = dev;
+  b->m.assign(m, m + count);
+  b->n.assign(n, n + count);
+  b->k.assign(k, k + count);
+  const fmm_plan* cls = classical_plan();
+  for (int i = 0; i < count; ++i) {
+    const fmm_plan* p = (plans && plans[i]) ? plans[i] : nullptr;
+    b->plans.push_back(p);
+    if (m[i] == 0 || n[i] == 0 || k[i] == 0) continue;
+    if (!p) {
+      batch_add_job(b, 0, i, cls, m[i], n[i], k[i], 0, 0, 0, 0, 0, 0);
+      continue;
+    }
+    // same partition and fringe regions as the single-problem path (run_fmm + peel)
+    const int pm = p->dims[0] * kMR, pk = p->dims[1], pn = p->dims[2] * kNR;
+    const int mr = m[i] % pm, kr = k[i] % pk, nr = n[i] % pn;
+    const int md = m[i] - mr, kd = k[i] - kr, nd = n[i] - nr;
+    if (md > 0 && nd > 0 && kd > 0)
+      batch_add_job(b, 0, i, p, md / p->dims[0], nd / p->dims[2], kd / p->dims[1], 0, 0, 0, 0, 0, 0);
+    if (kr > 0 && md > 0 && nd > 0) batch_add_job(b, 1, i, cls, md, nd, kr, 0, kd, kd, 0, 0, 0);
+    if (nr > 0) batch_add_job(b, 0, i, cls, m[i], nr, k[i], 0, 0, 0, nd, 0, nd);
+    if (mr > 0 && nd > 0) batch_add_job(b, 0, i, cls, mr, nd, k[i], md, 0, 0, 0, md, 0);
+  }
+  // Longest units first: the persistent grid takes units in order, so the short ones
+  // fill in at the end.
+  for (int ph = 0; ph < 2; ++ph) {
+    std::stable_sort(b->jobs[ph].begin(), b->jobs[ph].end(),
+                     [](const fmm_batch::Job& x, const fmm_batch::Job& y) { return x.cost > y.cost; });
+    long long acc = 0;
+    for (auto& j : b->jobs[ph]) {
+      b->unit_start[ph].push_back((int)acc);
+      acc += j.units;
+    }
+    if (acc > INT32_MAX) {
+      batch_free(b);
+      return FMM_E_UNSUPPORTED;
+    }
+    b->unit_start[ph].push_back((int)acc);
+  }
+  auto fail = [&](cudaError_t e) {
+    batch_free(b);
+    return cuda_status(e);
+  };
+  cudaError_t e = cudaSuccess;
+  for (int ph = 0; ph < 2 && e == cudaSuccess; ++ph) {
+    const size_t nj = b->jobs[ph].size();
+    if (nj == 0) continue;
+    for (auto& j : b->jobs[ph]) {
+      DevTables* d = nullptr;
+      rc = device_tables(j.plan, &d);
+      if (rc != FMM_OK) {
+        batch_free(b);
+        return rc;
+      }
+    }
+    e = cudaMalloc((void**)&b->d_jobs[ph], sizeof(fmm::GemmArgs) * nj);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_start[ph], sizeof(int) * (nj + 1));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_jobs[ph], sizeof(fmm::GemmArgs) * nj);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->d_start[ph], b->unit_start[ph].data(), sizeof(int) * (nj + 1), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && b->n_lincomb > 0) {
+    e = cudaMalloc((void**)&b->d_lc, sizeof(fmm::LincombTask) * b->n_lincomb);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_lc, sizeof(fmm::LincombTask) * b->n_lincomb);
+  }
+  if (e == cudaSuccess && b->n_tickets > 0) e = cudaMalloc((void**)&b->d_tickets, sizeof(int) * b->n_tickets);
+  if (e == cudaSuccess && b->ws_bytes > 0) e = cudaMalloc((void**)&b->d_ws, b->ws_bytes);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+  if (e != cudaSuccess) return fail(e);
+  *out = b;
+  return FMM_OK;
+}
+
+// Fill the job table of one phase for this call's operands; false if a problem cannot
+// use TMA staging (the phase then runs with cp.async staging).
+bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, const double* const* B,
+                const long* ldb, double* const* C, const long* ldc, int* n_lc) {
+  bool tma = true;
+  for (size_t q = 0; q < b->jobs[ph].size(); ++q) {
+    const fmm_batch::Job& j = b->jobs[ph][q];
+    const DevTables& d = j.plan->dev[b->dev];
+    fmm::GemmArgs a{};
+    const long long la = lda[j.prob], lb = ldb[j.prob], lc = ldc[j.prob];
+    a.A = A[j.prob] + j.a_r + (long long)j.a_c * la;
+    a.lda = la;
+    a.B = B[j.prob] + j.b_r + (long long)j.b_c * lb;
+    a.ldb = lb;
+    a.C = C[j.prob] + j.c_r + (long long)j.c_c * lc;
+    a.ldc = lc;
+    a.ms = j.ms;
+    a.ns = j.ns;
+    a.ks = j.ks;
+    a.nprod = j.plan->rank;
+    a.tiles_m = j.tiles_m;
+    a.tiles_n = j.tiles_n;
+    a.chunks = j.chunks;
+    a.mode = fmm::MODE_ACCUM_C;
+    a.tickets = j.chunks > 1 ? b->d_tickets + j.ticket_off : nullptr;
+    a.status = dev_status[b->dev];
+    const long long am = (long long)j.grid[0] * j.ms, ak = (long long)j.grid[1] * j.ks,
+                    bn = (long long)j.grid[2] * j.ns;
+    if (j.presum) {
+      const double* S = reinterpret_cast<const double*>(b->d_ws + j.ws_off);
+      const double* T = S + (size_t)j.ms * j.ks * j.nA;
+      a.prods = d.prods_ps;
+      a.terms = d.terms_ps;
+      a.Aw = S;
+      a.ldaw = j.ms;
+      a.Bw = T;
+      a.ldbw = j.ldT;
+      for (int side = 0; side < 2; ++side) {
+        const int ns = side == 0 ? j.nA : j.nB;
+        if (ns == 0) continue;
+        fmm::LincombTask& t = b->h_lc[(*n_lc)++];
+        t = fmm::LincombTask{};
+        t.nout = ns;
+        fmm::LincombArgs& l = t.a;
+        l.X = side == 0 ? a.A : a.B;
+        l.ldx = side == 0 ? la : lb;
+        l.rows = side == 0 ? j.ms : j.ks;
+        l.cols = side == 0 ? j.ks : j.ns;
+        l.blk_row_stride = l.rows;
+        l.blk_col_stride = l.cols;
+        l.out = const_cast<double*>(side == 0 ? S : T);
+        l.ldo = side == 0 ? j.ms : j.ldT;
+        l.out_stride = l.ldo * l.cols;
+        l.prods = d.prods;
+        l.terms = d.terms;
+        l.plist = side == 0 ? d.plistA : d.plistB;
+        l.side = side;
+      }
+    } else {
+      a.prods = d.prods;
+      a.terms = d.terms;
+      a.Aw = a.A;
+      a.ldaw = la;
+      a.Bw = a.B;
+      a.ldbw = lb;
+    }
+    bool ok = make_tensor_map(&a.tmA, a.A, am, ak, la, fmm::BM, fmm::BK) &&
+              make_tensor_map(&a.tmB, a.B, ak, bn, lb, fmm::BK, fmm::BN) &&
+              make_tensor_map(&a.tmB2, a.B, ak, bn, lb, fmm::TB_K, fmm::BN);
+    if (ok && j.presum && j.nA > 0)
+      ok = make_tensor_map(&a.tmAw, a.Aw, j.ms, (long long)j.nA * j.ks, j.ms, fmm::BM, fmm::BK);
+    else
+      a.tmAw = a.tmA;
+    if (ok && j.presum && j.nB > 0)
+      ok = make_tensor_map(&a.tmBw, a.Bw, j.ks, (long long)j.nB * j.ns, j.ldT, fmm::BK, fmm::BN) &&
+           make_tensor_map(&a.tmBw2, a.Bw, j.ks, (long long)j.nB * j.ns, j.ldT, fmm::TB_K, fmm::BN);
+    else
+      a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
+    tma = tma && ok;
+    b->h_jobs[ph][q] = a;
+  }
+  return tma;
+}
+
+int batch_run(fmm_batch* b, const double* const* A, const long* lda, const double* const* B, const long* ldb,
+              double* const* C, const long* ldc, cudaStream_t st) {
+  if (!b || !A || !lda || !B || !ldb || !C || !ldc) return FMM_E_INVALID;
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != b->dev) return FMM_E_INVALID;
+  for (int i = 0; i < b->count; ++i) {
+    int rc = check_args(b->m[i], b->n[i], b->k[i], A[i], lda[i], B[i], ldb[i], C[i], ldc[i]);
+    if (rc != FMM_OK) return rc;
+  }
+  // The staging buffers are reused: the previous call's copies out of them must be done.
+  // Inside a stream capture the copies become graph nodes that read the staging buffers
+  // at every replay, so a graph replays with the most recent call's operands.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  FMM_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+  if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventSynchronize(b->staged));
+  int n_lc = 0;
+  bool tma[2] = {true, true};
+  for (int ph = 0; ph < 2; ++ph)
+    if (!b->jobs[ph].empty()) tma[ph] = batch_fill(b, ph, A, lda, B, ldb, C, ldc, &n_lc);
+  for (int ph = 0; ph < 2; ++ph)
+    if (!b->jobs[ph].empty())
+      FMM_CUDA_TRY(cudaMemcpyAsync(b->d_jobs[ph], b->h_jobs[ph], sizeof(fmm::GemmArgs) * b->jobs[ph].size(),
+                                   cudaMemcpyHostToDevice, st));
+  if (n_lc > 0)
+    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_lc, b->h_lc, sizeof(fmm::LincombTask) * n_lc, cudaMemcpyHostToDevice, st));
+  if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventRecord(b->staged, st));
+  if (b->n_tickets > 0) FMM_CUDA_TRY(cudaMemsetAsync(b->d_tickets, 0, sizeof(int) * b->n_tickets, st));
+  if (n_lc > 0) {
+    ProfScope pf(K_LINCOMB_BATCH, st);
+    fmm::fmm_lincomb_batch_kernel<<<dim3(64, (unsigned)b->max_slots, (unsigned)n_lc), 256, 0, st>>>(b->d_lc);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
+  for (int ph = 0; ph < 2; ++ph) {
+    if (b->jobs[ph].empty()) continue;
+    fmm::BatchArgs ba{};
+    ba.jobs = b->d_jobs[ph];
+    ba.unit_start = b->d_start[ph];
+    ba.njobs = (int)b->jobs[ph].size();
+    ba.units = b->unit_start[ph].back();
+    ba.status = dev_status[b->dev];
+    const unsigned grid = (unsigned)std::min<long long>(ba.units, sm_count[b->dev]);
+    {
+      ProfScope pf(K_GEMM_BATCH, st);
+      if (tma[ph])
+        fmm::fmm_gemm_batch_kernel<true><<<grid, fmm::NTHREADS, fmm::smem_bytes(true), st>>>(ba);
+      else
+        fmm::fmm_gemm_batch_kernel<false><<<grid, fmm::NTHREADS, fmm::smem_bytes(false), st>>>(ba);
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
+  return FMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmm_batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k,
+                     fmm_batch** out) {
+  return batch_create(count, plans, m, n, k, out);
+}
+
+int fmm_batch_dgemm(fmm_batch* batch, const double* const* A, const long* lda, const double* const* B,
+                    const long* ldb, double* const* C, const long* ldc, void* stream) {
+  return batch_run(batch, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+}
+
+int fmm_batch_units(const fmm_batch* batch, int phase) {
+  if (!batch || phase < 0 || phase > 1) return FMM_E_INVALID;
+  return batch->unit_start[phase].empty() ? 0 : batch->unit_start[phase].back();
+}
+
+int fmm_batch_destroy(fmm_batch* batch) {
+  if (!batch) return FMM_E_INVALID;
+  cudaEventSynchronize(batch->staged);
+  batch_free(batch);
+  return FMM_OK;
+}
+
+}  // extern "C"

@@ -278,7 +278,9 @@ __device__ __forceinline__ int num_units(const GemmArgs& a) {
 // Producer: flattened stream of load units (k step s, term t) over the CTA's work units.
 // ------------------------------------------------------------------------------------
 struct LoadIter {
-  int u;            // work unit index (global)
+  int u;            // work unit index (global over the launch)
+  int j;            // problem of the unit (0 for a single-problem launch)
+  int nks;          // k steps per product of that problem
   Unit w;
   int r;            // product
   Prod p;
@@ -290,16 +292,60 @@ struct LoadIter {
   Term ta, tb;
 };
 
+// Where a launch's work units come from.  OneJob: one problem, the kernel parameter (its
+// fields stay in the parameter space).  JobBatch: many problems in global memory, problem
+// j owning the units [unit_start[j], unit_start[j + 1]).
+struct OneJob {
+  const GemmArgs& a;
+  __device__ __forceinline__ const GemmArgs& get(int) const { return a; }
+  __device__ __forceinline__ int find(int) const { return 0; }
+  __device__ __forceinline__ int first_unit(int) const { return 0; }
+  __device__ __forceinline__ int total() const { return num_units(a); }
+  __device__ __forceinline__ unsigned* status() const { return a.status; }
+  __device__ __forceinline__ void acquire_maps(int) const {}
+};
+
+struct JobBatch {
+  const GemmArgs* jobs;
+  const int* unit_start;
+  int njobs, units;
+  unsigned* st;
+  __device__ __forceinline__ const GemmArgs& get(int j) const { return jobs[j]; }
+  __device__ __forceinline__ int find(int u) const {  // last j with unit_start[j] <= u
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(unit_start + mid) <= u)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ int first_unit(int j) const { return __ldg(unit_start + j); }
+  __device__ __forceinline__ int total() const { return units; }
+  __device__ __forceinline__ unsigned* status() const { return st; }
+  // The tensor maps were written into global memory by a copy before the launch; order
+  // that write before the tensor-map proxy reads them.
+  __device__ __forceinline__ void acquire_maps(int j) const {
+    const CUtensorMap* m = &jobs[j].tmA;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m + q) : "memory");
+  }
+};
+
 __device__ __forceinline__ void load_terms(const GemmArgs& a, LoadIter& it) {
   if (it.t < it.p.na) it.ta = a.terms[it.p.a0 + it.t];
   if (it.t < it.p.nb) it.tb = a.terms[it.p.b0 + it.t];
 }
 
-__device__ __forceinline__ void load_iter_start(const GemmArgs& a, LoadIter& it, int nks) {
-  it.u = blockIdx.x;
-  it.valid = it.u < num_units(a) && nks > 0;
-  if (!it.valid) return;
-  it.w = decode_unit(a, it.u);
+template <class Src>
+__device__ __forceinline__ void iter_enter_unit(const Src& src, LoadIter& it) {
+  it.j = src.find(it.u);
+  const GemmArgs& a = src.get(it.j);
+  it.nks = (a.ks + BK - 1) / BK;
+  it.w = decode_unit(a, it.u - src.first_unit(it.j));
   it.r = it.w.r0;
   it.p = a.prods[it.r];
   it.T = prod_T(it.p);
@@ -308,13 +354,22 @@ __device__ __forceinline__ void load_iter_start(const GemmArgs& a, LoadIter& it,
   load_terms(a, it);
 }
 
-__device__ __forceinline__ void load_iter_next(const GemmArgs& a, LoadIter& it, int nks) {
+template <class Src>
+__device__ __forceinline__ void load_iter_start(const Src& src, LoadIter& it) {
+  it.u = blockIdx.x;
+  it.valid = it.u < src.total();
+  if (it.valid) iter_enter_unit(src, it);
+}
+
+template <class Src>
+__device__ __forceinline__ void load_iter_next(const Src& src, LoadIter& it) {
+  const GemmArgs& a = src.get(it.j);
   if (++it.t < it.T) {
     load_terms(a, it);
     return;
   }
   it.t = 0;
-  if (++it.s < nks) {
+  if (++it.s < it.nks) {
     if (it.T > 1) load_terms(a, it);
     return;
   }
@@ -326,15 +381,11 @@ __device__ __forceinline__ void load_iter_next(const GemmArgs& a, LoadIter& it, 
     return;
   }
   it.u += gridDim.x;
-  if (it.u >= num_units(a)) {
+  if (it.u >= src.total()) {
     it.valid = false;
     return;
   }
-  it.w = decode_unit(a, it.u);
-  it.r = it.w.r0;
-  it.p = a.prods[it.r];
-  it.T = prod_T(it.p);
-  load_terms(a, it);
+  iter_enter_unit(src, it);
 }
 
 // Raw slot layout (thread-private, conflict-free): pair e of A at [e][pt] (16 B each),
@@ -430,17 +481,18 @@ __device__ __forceinline__ void fold_unit(const LoadIter& it, const double* raw_
   }
 }
 
-__device__ __forceinline__ void producer(const GemmArgs& a, double* stages, double* raw, unsigned full0, unsigned empty0, int pt,
-                         int nks) {
+template <class Src>
+__device__ __forceinline__ void producer(const Src& src, double* stages, double* raw, unsigned full0, unsigned empty0,
+                                         int pt) {
   LoadIter iss, con;
-  load_iter_start(a, iss, nks);
-  load_iter_start(a, con, nks);
+  load_iter_start(src, iss);
+  load_iter_start(src, con);
   // prologue: NRAW - 1 load units in flight
 #pragma unroll 1
   for (int i = 0; i < NRAW - 1; ++i) {
     if (iss.valid) {
-      issue_unit(a, iss, raw + (size_t)(i % NRAW) * RAW_SZ, pt);
-      load_iter_next(a, iss, nks);
+      issue_unit(src.get(iss.j), iss, raw + (size_t)(i % NRAW) * RAW_SZ, pt);
+      load_iter_next(src, iss);
     }
     cp_async_commit();
   }
@@ -451,13 +503,13 @@ __device__ __forceinline__ void producer(const GemmArgs& a, double* stages, doub
     const int stage = (int)(kc % NSTAGE);
     double* opA = stages + (size_t)stage * STAGE_SZ;
     double* opB = opA + OPA_SZ;
-    if (con.t == 0) mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    if (con.t == 0) mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), src.status());
     cp_async_wait<NRAW - 2>();
     fold_unit(con, raw + (size_t)(unit % NRAW) * RAW_SZ, opA, opB, pt);
     const bool last_term = (con.t == con.T - 1);
     if (iss.valid) {
-      issue_unit(a, iss, raw + (size_t)((unit + NRAW - 1) % NRAW) * RAW_SZ, pt);
-      load_iter_next(a, iss, nks);
+      issue_unit(src.get(iss.j), iss, raw + (size_t)((unit + NRAW - 1) % NRAW) * RAW_SZ, pt);
+      load_iter_next(src, iss);
     }
     cp_async_commit();
     ++unit;
@@ -466,7 +518,7 @@ __device__ __forceinline__ void producer(const GemmArgs& a, double* stages, doub
       if ((pt & 31) == 0) mbar_arrive(full0 + 8 * stage);
       ++kc;
     }
-    load_iter_next(a, con, nks);
+    load_iter_next(src, con);
   }
   cp_async_wait<0>();
 }
@@ -495,13 +547,12 @@ __device__ __forceinline__ KStep kstep_info(const GemmArgs& a, const LoadIter& i
 }
 
 // Per-k-step iterator over (unit, product, k step); ta / tb hold the first A / B term.
-__device__ __forceinline__ void kiter_start(const GemmArgs& a, LoadIter& it, int nks) {
-  load_iter_start(a, it, nks);
-}
-__device__ __forceinline__ void kiter_next(const GemmArgs& a, LoadIter& it, int nks) {
+template <class Src>
+__device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it) {
   it.t = 0;
-  if (++it.s < nks) return;
+  if (++it.s < it.nks) return;
   it.s = 0;
+  const GemmArgs& a = src.get(it.j);
   if (++it.r < it.w.r1) {
     it.p = a.prods[it.r];
     it.T = prod_T(it.p);
@@ -509,29 +560,32 @@ __device__ __forceinline__ void kiter_next(const GemmArgs& a, LoadIter& it, int 
     return;
   }
   it.u += gridDim.x;
-  if (it.u >= num_units(a)) {
+  if (it.u >= src.total()) {
     it.valid = false;
     return;
   }
-  it.w = decode_unit(a, it.u);
-  it.r = it.w.r0;
-  it.p = a.prods[it.r];
-  it.T = prod_T(it.p);
-  load_terms(a, it);
+  iter_enter_unit(src, it);
 }
 
-__device__ __forceinline__ void tma_issuer(const GemmArgs& a, double* stages, double* raw, SlotMeta* meta, unsigned full0,
-                           unsigned empty0, unsigned rfull0, unsigned rempty0, int nks) {
+template <class Src>
+__device__ __forceinline__ void tma_issuer(const Src& src, double* stages, double* raw, SlotMeta* meta, unsigned full0,
+                                           unsigned empty0, unsigned rfull0, unsigned rempty0) {
   LoadIter it;
-  kiter_start(a, it, nks);
+  load_iter_start(src, it);
   long long kc = 0, rc = 0;
+  int mapped = -1;  // problem whose tensor maps were last acquired
 #pragma unroll 1
   while (it.valid) {
+    const GemmArgs& a = src.get(it.j);
+    if (it.j != mapped) {
+      src.acquire_maps(it.j);
+      mapped = it.j;
+    }
     const int stage = (int)(kc % NSTAGE);
     double* opA = stages + (size_t)stage * STAGE_SZ;
     const KStep ks = kstep_info(a, it);
     const int k0 = it.s * BK;
-    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), src.status());
     const unsigned fb = full0 + 8 * stage;
     mbar_arrive_expect_tx(fb, (ks.dirA ? TMA_BYTES_A : 0u) + (ks.dirB ? TMA_BYTES_B8 : 0u));
     if (ks.dirA)
@@ -543,7 +597,7 @@ __device__ __forceinline__ void tma_issuer(const GemmArgs& a, double* stages, do
 #pragma unroll 1
     for (int t = 0; t < ks.T; ++t, ++rc) {
       const int slot = (int)(rc % NRAW_TMA);
-      if (rc >= NRAW_TMA) mbar_wait(rempty0 + 8 * slot, (unsigned)(((rc / NRAW_TMA) - 1) & 1), a.status);
+      if (rc >= NRAW_TMA) mbar_wait(rempty0 + 8 * slot, (unsigned)(((rc / NRAW_TMA) - 1) & 1), src.status());
       const bool hasA = !ks.dirA && t < it.p.na, hasB = !ks.dirB && t < it.p.nb;
       const unsigned rb = rfull0 + 8 * slot;
       double* rs = raw + (size_t)slot * TRAW_SZ;
@@ -559,7 +613,7 @@ __device__ __forceinline__ void tma_issuer(const GemmArgs& a, double* stages, do
       if (hasB) tma_load_2d(smem_u32(rs + TRAW_A), tB.src ? &a.tmBw2 : &a.tmB2, xk & ~1, tB.col * a.ns + it.w.n0, rb);
     }
     ++kc;
-    kiter_next(a, it, nks);
+    kiter_next(src, it);
   }
 }
 
@@ -599,14 +653,16 @@ __device__ __forceinline__ void fold_slot(const double* rs, const SlotMeta& m, b
   }
 }
 
-__device__ __forceinline__ void tma_folder(const GemmArgs& a, double* stages, const double* raw, const SlotMeta* meta,
-                           unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft, int nks) {
+template <class Src>
+__device__ __forceinline__ void tma_folder(const Src& src, double* stages, const double* raw, const SlotMeta* meta,
+                                           unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft) {
   LoadIter it;
-  kiter_start(a, it, nks);
+  load_iter_start(src, it);
   long long kc = 0, rc = 0;
   const int lane = ft & 31;
 #pragma unroll 1
   while (it.valid) {
+    const GemmArgs& a = src.get(it.j);
     const int stage = (int)(kc % NSTAGE);
     double* opA = stages + (size_t)stage * STAGE_SZ;
     double* opB = opA + OPA_SZ;
@@ -616,14 +672,14 @@ __device__ __forceinline__ void tma_folder(const GemmArgs& a, double* stages, co
     // stage's full barrier, even when it has nothing to fold: an arrival made earlier
     // could land in the barrier's previous phase (whose issuer arrival and bytes may
     // still be outstanding) and break that phase's transaction accounting.
-    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), a.status);
+    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE) & 1) ^ 1), src.status());
     if (ks.T > 0) {
       double2 accA[FPAIRS];
       double accB[FELEMS];
 #pragma unroll 1
       for (int t = 0; t < ks.T; ++t, ++rc) {
         const int slot = (int)(rc % NRAW_TMA);
-        mbar_wait(rfull0 + 8 * slot, (unsigned)((rc / NRAW_TMA) & 1), a.status);
+        mbar_wait(rfull0 + 8 * slot, (unsigned)((rc / NRAW_TMA) & 1), src.status());
         const double* rs = raw + (size_t)slot * TRAW_SZ;
         const bool hasA = !ks.dirA && t < it.p.na, hasB = !ks.dirB && t < it.p.nb;
         if (kvalid >= BK)
@@ -658,7 +714,7 @@ __device__ __forceinline__ void tma_folder(const GemmArgs& a, double* stages, co
     __syncwarp();
     if (lane == 0) mbar_arrive(full0 + 8 * stage);
     ++kc;
-    kiter_next(a, it, nks);
+    kiter_next(src, it);
   }
 }
 
@@ -784,19 +840,25 @@ __device__ __forceinline__ void ticket_release(const GemmArgs& a, int tile, int 
   if (ct == 0) st_release(a.tickets + tile, chunk + 1);
 }
 
-__device__ __forceinline__ void consumer(const GemmArgs& a, const double* stages, unsigned full0, unsigned empty0, int ct, int nks) {
+template <class Src>
+__device__ __forceinline__ void consumer(const Src& src, const double* stages, unsigned full0, unsigned empty0,
+                                         int ct) {
   const int warp = ct >> 5, lane = ct & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
-  const int nunits = num_units(a);
-  const int ntiles = a.tiles_m * a.tiles_n;
-  const bool ordered = (a.mode == MODE_ACCUM_C) && a.chunks > 1;
+  const int nunits = src.total();
   long long kc = 0;
   double acc[4][4][4];
 #pragma unroll 1
   for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-    const Unit w = decode_unit(a, u);
-    const int chunk = u / ntiles;
+    const int job = src.find(u);
+    const GemmArgs& a = src.get(job);
+    const int ul = u - src.first_unit(job);
+    const int ntiles = a.tiles_m * a.tiles_n;
+    const bool ordered = (a.mode == MODE_ACCUM_C) && a.chunks > 1;
+    const int nks = (a.ks + BK - 1) / BK;
+    const Unit w = decode_unit(a, ul);
+    const int chunk = ul / ntiles;
 #pragma unroll 1
     for (int r = w.r0; r < w.r1; ++r) {
       const Prod p = a.prods[r];
@@ -811,7 +873,7 @@ __device__ __forceinline__ void consumer(const GemmArgs& a, const double* stages
         const int stage = (int)(kc % NSTAGE);
         const double* opA = stages + (size_t)stage * STAGE_SZ;
         const double* opB = opA + OPA_SZ;
-        mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), a.status);
+        mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), src.status());
         if (s == nks - C_PREFETCH_STEPS) prefetch_c_tiles(a, p, w.m0, w.n0, ct);
         mma_stage(opA, opB, acc, wm, wn, g, t4);
         // The stage is refilled by TMA as soon as every warp has arrived; the fence
@@ -832,8 +894,8 @@ __device__ __forceinline__ void consumer(const GemmArgs& a, const double* stages
 // Persistent: one CTA per SM walks work units blockIdx.x, blockIdx.x + gridDim.x, ...
 // TMA = true stages operands with tensor copies (A, B 16-byte aligned, even leading
 // dimensions); TMA = false with per-thread cp.async (any alignment).
-template <bool TMA>
-__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_constant__ GemmArgs a) {
+template <bool TMA, class Src>
+__device__ __forceinline__ void gemm_cta(const Src& src) {
   extern __shared__ __align__(128) double smem[];
   double* stages = smem;                                  // [NSTAGE][STAGE_SZ]
   double* raw = stages + (size_t)NSTAGE * STAGE_SZ;       // [NRAW][RAW_SZ] or [NRAW_TMA][TRAW_SZ]
@@ -859,21 +921,41 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_cons
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  const int nks = (a.ks + BK - 1) / BK;
   if (tid < NPROD) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
     if (TMA) {
       if (tid == 0)
-        tma_issuer(a, stages, raw, meta, full0, empty0, rfull0, rempty0, nks);
+        tma_issuer(src, stages, raw, meta, full0, empty0, rfull0, rempty0);
       else if (tid >= 32)
-        tma_folder(a, stages, raw, meta, full0, empty0, rfull0, rempty0, tid - 32, nks);
+        tma_folder(src, stages, raw, meta, full0, empty0, rfull0, rempty0, tid - 32);
     } else {
-      producer(a, stages, raw, full0, empty0, tid, nks);
+      producer(src, stages, raw, full0, empty0, tid);
     }
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
-    consumer(a, stages, full0, empty0, tid - NPROD, nks);
+    consumer(src, stages, full0, empty0, tid - NPROD);
   }
+}
+
+template <bool TMA>
+__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_kernel(const __grid_constant__ GemmArgs a) {
+  gemm_cta<TMA>(OneJob{a});
+}
+
+// Many independent problems (each with its own plan tables, operands, sizes, tensor maps
+// and tickets) in one persistent launch: the units of all problems form one sequence,
+// problem j owning [unit_start[j], unit_start[j + 1]).
+struct BatchArgs {
+  const GemmArgs* jobs;    // global memory, 64-byte aligned (tensor maps inside)
+  const int* unit_start;   // njobs + 1 entries
+  int njobs;
+  int units;
+  unsigned* status;
+};
+
+template <bool TMA>
+__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_batch_kernel(const BatchArgs b) {
+  gemm_cta<TMA>(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status});
 }
 
 // Operand sums in HBM: out_j = sum_t coef_t * X_{blk_t} for the A terms (side 0) or the
@@ -896,8 +978,7 @@ struct LincombArgs {
   int side;
 };
 
-__global__ void fmm_lincomb_kernel(const LincombArgs a) {
-  const int j = blockIdx.y;
+__device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j) {
   const int r = a.plist ? a.plist[j] : j;
   const Prod p = a.prods[r];
   const int t0 = a.side == 0 ? p.a0 : p.b0;
@@ -934,6 +1015,22 @@ __global__ void fmm_lincomb_kernel(const LincombArgs a) {
       if (two) o[1] = v1;
     }
   }
+}
+
+__global__ void fmm_lincomb_kernel(const LincombArgs a) { lincomb_body(a, blockIdx.y); }
+
+// The operand sums of many problems in one launch: task blockIdx.z, output blockIdx.y
+// (tasks with fewer outputs return at once), elements grid-strided over blockIdx.x.
+struct LincombTask {
+  LincombArgs a;
+  int nout;
+  int pad;
+};
+
+__global__ void fmm_lincomb_batch_kernel(const LincombTask* tasks) {
+  const LincombTask& tk = tasks[blockIdx.z];
+  if ((int)blockIdx.y >= tk.nout) return;
+  lincomb_body(tk.a, blockIdx.y);
 }
 
 // M_Add: C_l += sum_r W[l, r] * M_r for every C block l, products applied in order r.

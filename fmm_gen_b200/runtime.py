@@ -87,6 +87,15 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_split_gemm_dev.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_long, c_void_p, c_long, c_void_p,
                                        c_long, c_void_p]
     lib.fmm_split_gemm_dev.restype = c_int
+    lib.fmm_batch_create.argtypes = [c_int, ctypes.POINTER(c_void_p), c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p)]
+    lib.fmm_batch_create.restype = c_int
+    lib.fmm_batch_dgemm.argtypes = [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_long), ctypes.POINTER(c_void_p),
+                                    ctypes.POINTER(c_long), ctypes.POINTER(c_void_p), ctypes.POINTER(c_long), c_void_p]
+    lib.fmm_batch_dgemm.restype = c_int
+    lib.fmm_batch_units.argtypes = [c_void_p, c_int]
+    lib.fmm_batch_units.restype = c_int
+    lib.fmm_batch_destroy.argtypes = [c_void_p]
+    lib.fmm_batch_destroy.restype = c_int
     for name in ("bl_dgemm", "bl_dgemm_strassen_abc", "bl_dgemm_strassen_ab", "bl_dgemm_strassen_naive"):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]
@@ -237,6 +246,69 @@ def split_gemm(plan, A, B, C, stream=None) -> None:
     rc = lib.fmm_split_gemm_dev(plan.handle if plan is not None else None, m, n, k, A.data_ptr(), _ld(A, m),
                                 B.data_ptr(), _ld(B, k), C.data_ptr(), _ld(C, m), ctypes.c_void_p(s.cuda_stream))
     _check(rc, "fmm_split_gemm_dev")
+
+
+class Batch:
+    """Many independent FP64 problems C_i += A_i @ B_i in one persistent launch.
+
+    `shapes` is a list of (m, n, k); `plans[i]` is a Plan or None (classical).  Creating a
+    batch fixes the shapes and plans, splits every problem into its FMM core and fringe
+    strips (the same partition as fmm_gemm), orders the work units longest first and
+    allocates the job tables, tickets and pre-summed operand workspaces once.  `run`
+    then takes this call's operands (column-major float64 CUDA tensors) and enqueues
+    the launch on the current stream; it can be captured in a CUDA graph (the graph
+    replays with the operand pointers of the captured call)."""
+
+    def __init__(self, shapes, plans=None):
+        self._lib = load_library()
+        shapes = [tuple(int(v) for v in s) for s in shapes]
+        if not shapes:
+            raise FmmError(-1, "empty batch")
+        count = len(shapes)
+        plans = list(plans) if plans is not None else [None] * count
+        if len(plans) != count:
+            raise FmmError(-1, "plans and shapes differ in length")
+        self.shapes, self.plans = shapes, plans
+        ci = ctypes.c_int * count
+        handles = (ctypes.c_void_p * count)(*[p.handle if p is not None else None for p in plans])
+        h = ctypes.c_void_p()
+        _check(self._lib.fmm_batch_create(count, handles, ci(*[s[0] for s in shapes]), ci(*[s[1] for s in shapes]),
+                                          ci(*[s[2] for s in shapes]), ctypes.byref(h)), "fmm_batch_create")
+        self.handle = h
+
+    def units(self, phase: int = 0) -> int:
+        return int(self._lib.fmm_batch_units(self.handle, phase))
+
+    def run(self, As, Bs, Cs, stream=None) -> None:
+        import torch
+
+        count = len(self.shapes)
+        if not (len(As) == len(Bs) == len(Cs) == count):
+            raise FmmError(-1, "operand lists must match the batch size")
+        vp, cl = ctypes.c_void_p * count, ctypes.c_long * count
+        pa, pb, pc, la, lb, lc = [], [], [], [], [], []
+        for (m, n, k), A, B, C in zip(self.shapes, As, Bs, Cs):
+            if (tuple(A.shape), tuple(B.shape), tuple(C.shape)) != ((m, k), (k, n), (m, n)):
+                raise FmmError(-1, f"operands do not match the batch shape {(m, n, k)}")
+            _check_operands(A, B, C)
+            pa.append(A.data_ptr()); la.append(_ld(A, m))
+            pb.append(B.data_ptr()); lb.append(_ld(B, k))
+            pc.append(C.data_ptr()); lc.append(_ld(C, m))
+        s = stream if stream is not None else torch.cuda.current_stream()
+        rc = self._lib.fmm_batch_dgemm(self.handle, vp(*pa), cl(*la), vp(*pb), cl(*lb), vp(*pc), cl(*lc),
+                                       ctypes.c_void_p(s.cuda_stream))
+        _check(rc, "fmm_batch_dgemm")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.fmm_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # --------------------------------------------------------------------------------

@@ -133,6 +133,32 @@ int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const doubl
 int fmm_split_gemm_dev(const fmm_plan *plan, int m, int n, int k, const float *A, long lda, const float *B,
                        long ldb, double *C, long ldc, void *stream);
 
+/* ---- batches: many independent problems in one persistent launch ----
+ * The reference runs one generated entry point per call (meta/abc_gen_mix.py:448-472);
+ * a batch runs many problems C_i += A_i * B_i (FP64, column-major), each with its own
+ * plan (NULL = classical), in one persistent launch of the FMM kernel whose work units
+ * span every problem, longest units first.  Each problem is partitioned exactly as
+ * fmm_dgemm_dev partitions it (FMM core plus fringe strips), so results are identical
+ * to calling fmm_dgemm_dev per problem.  A second launch handles the k-fringe strips
+ * (they update the same C region as their core), and a launch before them forms the
+ * pre-summed operands of the large FMM problems.
+ *
+ * fmm_batch_create fixes the shapes and plans and allocates (cudaMalloc) the job tables,
+ * tickets and workspaces; the plans must outlive the batch.  fmm_batch_dgemm takes this
+ * call's device pointers and enqueues the work on `stream` without allocating; it may be
+ * captured in a CUDA graph.  The job tables go to the device from host staging buffers
+ * owned by the batch, so a graph replays with the operands of the batch's most recent
+ * fmm_batch_dgemm call (the captured one, unless the batch was called again since).
+ * Destroy a batch only after its work has completed. */
+typedef struct fmm_batch fmm_batch;
+int fmm_batch_create(int count, const fmm_plan *const *plans, const int *m, const int *n, const int *k,
+                     fmm_batch **out);
+int fmm_batch_dgemm(fmm_batch *batch, const double *const *A, const long *lda, const double *const *B,
+                    const long *ldb, double *const *C, const long *ldc, void *stream);
+/* Work units of the main launch (phase 0) or of the k-fringe launch (phase 1). */
+int fmm_batch_units(const fmm_batch *batch, int phase);
+int fmm_batch_destroy(fmm_batch *batch);
+
 /* Number of kernels the library launched since load (all entry points, all streams). */
 long long fmm_kernel_launch_count(void);
 
