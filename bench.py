@@ -166,6 +166,138 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def split_bf16_8192(rt, torch, dev, steps=3):
+    """Split-BF16 FMM (222-2, 8192^3): FP32 inputs in two sets (N(0,1); log-uniform
+    magnitudes 2^-10..2^10 with random sign), FP64 C; time, effective TFLOPS against the
+    project's plain FP64 GEMM on the same values, and the relative Frobenius error against
+    an FP64 classical GEMM (cuBLAS) of the same inputs."""
+    n = 8192
+    p2 = rt.Plan.from_levels(["222"], [2])
+    g = torch.Generator(device=dev).manual_seed(8192)
+    out = {"algorithm": "222-2", "shape": [n, n, n], "products": "6 bf16 plane products, FP32 accumulate, FP64 scatter"}
+
+    def loguniform():
+        e = torch.empty((n, n), device=dev).uniform_(-10, 10, generator=g)
+        s = torch.empty((n, n), device=dev).uniform_(-1, 1, generator=g).sign()
+        return rt.colmajor(n, n, dtype=torch.float32, device=dev).copy_(s * torch.exp2(e))
+
+    sets = {
+        "normal": lambda: rt.colmajor(n, n, dtype=torch.float32, device=dev).normal_(generator=g),
+        "loguniform": loguniform,
+    }
+    C = rt.colmajor(n, n, device=dev)
+    f = 2.0 * n ** 3
+    for name, make in sets.items():
+        A, B = make(), make()
+        C.zero_()
+        rt.split_gemm(p2, A, B, C)
+        torch.cuda.synchronize()
+        ref = A.double() @ B.double()
+        err = ((C - ref).norm() / ref.norm()).item()
+        del ref
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            rt.split_gemm(p2, A, B, C)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms": ms, "tflops_effective": f / (ms * 1e-3) / 1e12, "rel_fro_err": err}
+        del A, B
+    # the plain FP64 comparator on FP64 operands of the same size
+    Ad = rt.colmajor(n, n, device=dev).uniform_(-1, 1, generator=g)
+    Bd = rt.colmajor(n, n, device=dev).uniform_(-1, 1, generator=g)
+    rt.plain_gemm(Ad, Bd, C)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        rt.plain_gemm(Ad, Bd, C)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / steps
+    out["plain_fp64_ms"] = plain_ms
+    out["speedup_vs_plain_fp64"] = {k: plain_ms / out[k]["ms"] for k in sets}
+    with rt.KernelTimer() as kt:
+        rt.split_gemm(p2, Ad.float(), Bd.float(), C)
+    out["kernel_ms"] = {k: v for k, v in kt.ms.items() if kt.count[k]}
+    peak = _measured_peak("bf16_tflops")
+    gemm_ms = kt.ms.get("fmm_split_gemm_kernel", 0.0)
+    if gemm_ms > 0:
+        bf16_flops = 49 * 6 * 2.0 * (n // 4) ** 3
+        ach = bf16_flops / (gemm_ms * 1e-3) / 1e12
+        out["roofline"] = {"bound": "tensor", "kernel": "fmm_split_gemm_kernel", "achieved": ach, "peak": peak,
+                           "unit": "TFLOP/s", "frac": ach / peak if peak else None,
+                           "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"}
+    del Ad, Bd, C
+    torch.cuda.empty_cache()
+    return out
+
+
+def _measured_peak(key):
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)[key])
+    except Exception:
+        return None
+
+
+def batch_512(rt, torch, dev, steps=3):
+    """512 FP64 problems, m, n, k log-uniform in [256, 4096] from the seed, entries U(-1,1),
+    C += A*B in one persistent launch (captured in a CUDA graph and replayed); per-problem
+    algorithm from the tuner (model seed, then measured refinement)."""
+    from fmm_gen_b200 import tuner
+
+    shapes = tuner.random_batch_shapes(512, seed=0)
+    g = torch.Generator(device=dev).manual_seed(512)
+    As, Bs, Cs = [], [], []
+    for (m, n, k) in shapes:
+        As.append(rt.colmajor(m, k, device=dev).uniform_(-1, 1, generator=g))
+        Bs.append(rt.colmajor(k, n, device=dev).uniform_(-1, 1, generator=g))
+        Cs.append(rt.colmajor(m, n, device=dev).uniform_(-1, 1, generator=g))
+    flops = sum(2.0 * m * n * k for (m, n, k) in shapes)
+    measure = tuner.batch_timer(rt, shapes, As, Bs, Cs, reps=2)
+    t0 = time.perf_counter()
+    tn = tuner.BatchTuner()
+    rep = tn.tune(shapes, measure)
+    tune_s = time.perf_counter() - t0
+    model_ms = sum(tuner.model_time(tn.model, c, *s) for c, s in zip(rep.choices, shapes)) * 1e3
+    classical_ms = measure(["classical"] * len(shapes))
+    for c in set(rep.choices) - {"classical"} - set(measure.plans):
+        measure.plans[c] = rt.Plan.from_levels(*tuner.candidate_levels(c))
+    plans = [None if c == "classical" else measure.plans[c] for c in rep.choices]
+    batch = rt.Batch(shapes, plans)
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        batch.run(As, Bs, Cs, stream=s)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        batch.run(As, Bs, Cs)
+    graph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with rt.KernelTimer() as kt:
+        e0.record()
+        for _ in range(steps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del graph
+    batch.close()
+    out = {"problems": len(shapes), "dims": "log-uniform [256, 4096], seed 0", "total_flop": flops,
+           "ms": ms, "tflops_effective": flops / (ms * 1e-3) / 1e12,
+           "all_classical_ms": classical_ms, "model_ms": model_ms,
+           "choices": rep.counts(), "tune_s": tune_s, "tune_trials": rep.trials,
+           "launches_per_replay": {k: v / steps for k, v in kt.count.items() if v}}
+    del As, Bs, Cs
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +305,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the split-BF16 and batch measurements")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -324,6 +457,13 @@ def main():
     e2e_value = world * eff * args.steps / float(te.item()) / 1e12
     del host
 
+    extra = {}
+    if not args.no_extra:
+        del mats
+        torch.cuda.empty_cache()
+        extra["split_bf16_222_2_8192"] = split_bf16_8192(rt, torch, dev)
+        extra["batch_512_fp64"] = batch_512(rt, torch, dev)
+
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, ts = oracle_sample_tflops(CPU_SAMPLE)
@@ -359,6 +499,7 @@ def main():
                                      "ratio": s_plain16 / s222},
             "rel_fro_err_vs_cublas": errs,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

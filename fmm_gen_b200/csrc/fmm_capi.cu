@@ -45,12 +45,14 @@ enum KernelKind {
   K_GEMM_SPLIT = 5,
   K_GEMM_BATCH = 6,
   K_LINCOMB_BATCH = 7,
-  K_NUM = 8
+  K_PITCH_COPY = 8,
+  K_NUM = 9
 };
 const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
                                          "fmm_lincomb_kernel", "fmm_scatter_kernel",
                                          "fmm_split_operands_kernel", "fmm_split_gemm_kernel",
-                                         "fmm_gemm_batch_kernel", "fmm_lincomb_batch_kernel"};
+                                         "fmm_gemm_batch_kernel", "fmm_lincomb_batch_kernel",
+                                         "fmm_pitch_copy_kernel"};
 struct ProfRec {
   int kind;
   cudaEvent_t e0, e1;
@@ -700,21 +702,23 @@ int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, co
   if (!plain && !plan) return FMM_E_NOPLAN;
   cudaStream_t st = cudaStreamPerThread;
   double *dA = nullptr, *dB = nullptr, *dC = nullptr;
-  const size_t szA = sizeof(double) * (size_t)m * k, szB = sizeof(double) * (size_t)k * n,
+  // even device pitches for A and B: tensor copies need 16-byte column starts
+  const int pa = m + (m & 1), pb = k + (k & 1);
+  const size_t szA = sizeof(double) * (size_t)pa * k, szB = sizeof(double) * (size_t)pb * n,
                szC = sizeof(double) * (size_t)m * n;
   FMM_CUDA_TRY(cudaMallocAsync((void**)&dA, szA, st));
   FMM_CUDA_TRY(cudaMallocAsync((void**)&dB, szB, st));
   FMM_CUDA_TRY(cudaMallocAsync((void**)&dC, szC, st));
-  FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, sizeof(double) * m, A, sizeof(double) * lda, sizeof(double) * m, k,
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, sizeof(double) * pa, A, sizeof(double) * lda, sizeof(double) * m, k,
                                  cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, sizeof(double) * k, B, sizeof(double) * ldb, sizeof(double) * k, n,
+  FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, sizeof(double) * pb, B, sizeof(double) * ldb, sizeof(double) * k, n,
                                  cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, sizeof(double) * m, C, sizeof(double) * ldc, sizeof(double) * m, n,
                                  cudaMemcpyHostToDevice, st));
   if (plain)
-    rc = plain_gemm(m, n, k, dA, m, dB, k, dC, m, st);
+    rc = plain_gemm(m, n, k, dA, pa, dB, pb, dC, m, st);
   else
-    rc = run_fmm(plan, pack, m, n, k, dA, m, dB, k, dC, m, st);
+    rc = run_fmm(plan, pack, m, n, k, dA, pa, dB, pb, dC, m, st);
   if (rc == FMM_OK)
     rc = cuda_status(cudaMemcpy2DAsync(C, sizeof(double) * ldc, dC, sizeof(double) * m, sizeof(double) * m, n,
                                        cudaMemcpyDeviceToHost, st));
@@ -725,6 +729,56 @@ int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, co
   if (rc == FMM_OK) rc = cuda_status(se);
   if (rc == FMM_OK) rc = device_status(true);
   return rc;
+}
+
+// Operands whose leading dimension is odd cannot be staged by tensor copies (columns
+// must start on 16 bytes) and fall back to per-thread copies at about half the speed.
+// Large ones are copied once, stream-ordered, into an even-pitch workspace instead
+// (bandwidth-bound, a few percent of the GEMM); small ones stay in place.
+constexpr long long kRepitchMinElems = 1LL << 18;
+
+struct Repitched {
+  const double* A;
+  long long lda;
+  const double* B;
+  long long ldb;
+  char* ws = nullptr;
+};
+
+int repitch(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, cudaStream_t st,
+            Repitched* out) {
+  out->A = A;
+  out->lda = lda;
+  out->B = B;
+  out->ldb = ldb;
+  const bool a_odd = (lda & 1) && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (long long)m * k >= kRepitchMinElems;
+  const bool b_odd = (ldb & 1) && (reinterpret_cast<uintptr_t>(B) & 15) == 0 && (long long)k * n >= kRepitchMinElems;
+  if (!a_odd && !b_odd) return FMM_OK;
+  const long long pa = m + (m & 1), pb = k + (k & 1);
+  const size_t sa = a_odd ? ((sizeof(double) * (size_t)pa * k + 255) & ~(size_t)255) : 0;
+  const size_t sb = b_odd ? sizeof(double) * (size_t)pb * n : 0;
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&out->ws, sa + sb, st));
+  if (a_odd) {
+    double* dst = reinterpret_cast<double*>(out->ws);
+    fmm::fmm_pitch_copy1_kernel<<<256, 256, 0, st>>>(fmm::PitchCopy{A, lda, dst, pa, m, k});
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    out->A = dst;
+    out->lda = pa;
+  }
+  if (b_odd) {
+    double* dst = reinterpret_cast<double*>(out->ws + sa);
+    fmm::fmm_pitch_copy1_kernel<<<256, 256, 0, st>>>(fmm::PitchCopy{B, ldb, dst, pb, k, n});
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    out->B = dst;
+    out->ldb = pb;
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+int release(Repitched& r, int rc, cudaStream_t st) {
+  if (!r.ws) return rc;
+  cudaError_t e = cudaFreeAsync(r.ws, st);
+  return rc == FMM_OK ? cuda_status(e) : rc;
 }
 
 }  // namespace
@@ -773,14 +827,24 @@ fmm_plan* fmm_default_plan(void) {
 
 int fmm_dgemm_dev(const fmm_plan* plan, int pack_type, int m, int n, int k, const double* A, long lda,
                   const double* B, long ldb, double* C, long ldc, void* stream) {
-  return run_fmm(plan, pack_type, m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
+  if (rc != FMM_OK || m == 0 || n == 0 || k == 0 || !plan) return run_fmm(plan, pack_type, m, n, k, A, lda, B, ldb, C, ldc, st);
+  Repitched r;
+  rc = repitch(m, n, k, A, lda, B, ldb, st, &r);
+  if (rc == FMM_OK) rc = run_fmm(plan, pack_type, m, n, k, r.A, r.lda, r.B, r.ldb, C, ldc, st);
+  return release(r, rc, st);
 }
 
 int fmm_plain_dgemm_dev(int m, int n, int k, const double* A, long lda, const double* B, long ldb, double* C,
                         long ldc, void* stream) {
   int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
-  if (rc != FMM_OK) return rc;
-  return plain_gemm(m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+  if (rc != FMM_OK || m == 0 || n == 0 || k == 0) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Repitched r;
+  rc = repitch(m, n, k, A, lda, B, ldb, st, &r);
+  if (rc == FMM_OK) rc = plain_gemm(m, n, k, r.A, r.lda, r.B, r.ldb, C, ldc, st);
+  return release(r, rc, st);
 }
 
 int fmm_dgemm_host(const fmm_plan* plan, int pack_type, int m, int n, int k, const double* A, int lda,
@@ -817,21 +881,22 @@ void bl_dynamic_peeling(int m, int n, int k, double* A, int lda, double* B, int 
   }
   cudaStream_t st = cudaStreamPerThread;
   double *dA = nullptr, *dB = nullptr, *dC = nullptr;
-  const size_t szA = sizeof(double) * (size_t)m * k, szB = sizeof(double) * (size_t)k * n,
+  const int pa = m + (m & 1), pb = k + (k & 1);  // even device pitches (16-byte column starts)
+  const size_t szA = sizeof(double) * (size_t)pa * k, szB = sizeof(double) * (size_t)pb * n,
                szC = sizeof(double) * (size_t)m * n;
   rc = cuda_status(cudaMallocAsync((void**)&dA, szA, st));
   if (rc == FMM_OK) rc = cuda_status(cudaMallocAsync((void**)&dB, szB, st));
   if (rc == FMM_OK) rc = cuda_status(cudaMallocAsync((void**)&dC, szC, st));
   if (rc == FMM_OK)
-    rc = cuda_status(cudaMemcpy2DAsync(dA, sizeof(double) * m, A, sizeof(double) * lda, sizeof(double) * m, k,
+    rc = cuda_status(cudaMemcpy2DAsync(dA, sizeof(double) * pa, A, sizeof(double) * lda, sizeof(double) * m, k,
                                        cudaMemcpyHostToDevice, st));
   if (rc == FMM_OK)
-    rc = cuda_status(cudaMemcpy2DAsync(dB, sizeof(double) * k, B, sizeof(double) * ldb, sizeof(double) * k, n,
+    rc = cuda_status(cudaMemcpy2DAsync(dB, sizeof(double) * pb, B, sizeof(double) * ldb, sizeof(double) * k, n,
                                        cudaMemcpyHostToDevice, st));
   if (rc == FMM_OK)
     rc = cuda_status(cudaMemcpy2DAsync(dC, sizeof(double) * m, C, sizeof(double) * ldc, sizeof(double) * m, n,
                                        cudaMemcpyHostToDevice, st));
-  if (rc == FMM_OK) rc = peel(m, n, k, dA, m, dB, k, dC, m, dim1, dim2, dim3, st);
+  if (rc == FMM_OK) rc = peel(m, n, k, dA, pa, dB, pb, dC, m, dim1, dim2, dim3, st);
   if (rc == FMM_OK)
     rc = cuda_status(cudaMemcpy2DAsync(C, sizeof(double) * ldc, dC, sizeof(double) * m, sizeof(double) * m, n,
                                        cudaMemcpyDeviceToHost, st));
@@ -1287,6 +1352,14 @@ struct fmm_batch {
   fmm::LincombTask* h_lc = nullptr;
   int* d_tickets = nullptr;
   char* d_ws = nullptr;
+  // Even-pitch copies of A / B for problems whose row count is odd (a dense operand then
+  // has an odd leading dimension, which tensor copies cannot stage): byte offsets into
+  // d_pitch, or SIZE_MAX when the operand needs none.
+  std::vector<size_t> pitch_a, pitch_b;
+  size_t pitch_bytes = 0;
+  char* d_pitch = nullptr;
+  fmm::PitchCopy* d_pc = nullptr;
+  fmm::PitchCopy* h_pc = nullptr;
   cudaEvent_t staged = nullptr;    // the staging buffers' last copies are done
 };
 
@@ -1365,6 +1438,9 @@ void batch_free(fmm_batch* b) {
   if (b->h_lc) cudaFreeHost(b->h_lc);
   if (b->d_tickets) cudaFree(b->d_tickets);
   if (b->d_ws) cudaFree(b->d_ws);
+  if (b->d_pitch) cudaFree(b->d_pitch);
+  if (b->d_pc) cudaFree(b->d_pc);
+  if (b->h_pc) cudaFreeHost(b->h_pc);
   if (b->staged) cudaEventDestroy(b->staged);
   delete b;
 }
@@ -1387,7 +1463,15 @@ int batch_create(int count, const fmm_plan* const* plans, const int* m, const in
   for (int i = 0; i < count; ++i) {
     const fmm_plan* p = (plans && plans[i]) ? plans[i] : nullptr;
     b->plans.push_back(p);
-    if (m[i] == 0 || n[i] == 0 || k[i] == 0) continue;
+    const bool live = m[i] > 0 && n[i] > 0 && k[i] > 0;
+    auto reserve = [&](int rows, int cols) {
+      const size_t off = b->pitch_bytes;
+      b->pitch_bytes += (sizeof(double) * (size_t)(rows + 1) * cols + 255) & ~(size_t)255;
+      return off;
+    };
+    b->pitch_a.push_back(live && (m[i] & 1) ? reserve(m[i], k[i]) : SIZE_MAX);
+    b->pitch_b.push_back(live && (k[i] & 1) ? reserve(k[i], n[i]) : SIZE_MAX);
+    if (!live) continue;
     if (!p) {
       batch_add_job(b, 0, i, cls, m[i], n[i], k[i], 0, 0, 0, 0, 0, 0);
       continue;
@@ -1446,6 +1530,11 @@ int batch_create(int count, const fmm_plan* const* plans, const int* m, const in
   }
   if (e == cudaSuccess && b->n_tickets > 0) e = cudaMalloc((void**)&b->d_tickets, sizeof(int) * b->n_tickets);
   if (e == cudaSuccess && b->ws_bytes > 0) e = cudaMalloc((void**)&b->d_ws, b->ws_bytes);
+  if (e == cudaSuccess && b->pitch_bytes > 0) {
+    e = cudaMalloc((void**)&b->d_pitch, b->pitch_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_pc, sizeof(fmm::PitchCopy) * 2 * count);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_pc, sizeof(fmm::PitchCopy) * 2 * count);
+  }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(e);
   *out = b;
@@ -1552,18 +1641,46 @@ int batch_run(fmm_batch* b, const double* const* A, const long* lda, const doubl
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   FMM_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
   if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventSynchronize(b->staged));
+  // Operands with an odd leading dimension and a reserved even-pitch copy are staged
+  // through it (rows + 1 pitch); the others are used in place.
+  std::vector<const double*> eA(A, A + b->count), eB(B, B + b->count);
+  std::vector<long> elda(lda, lda + b->count), eldb(ldb, ldb + b->count);
+  int n_pc = 0;
+  for (int i = 0; i < b->count; ++i) {
+    if ((lda[i] & 1) && b->pitch_a[i] != SIZE_MAX) {
+      double* dst = reinterpret_cast<double*>(b->d_pitch + b->pitch_a[i]);
+      b->h_pc[n_pc++] = fmm::PitchCopy{A[i], lda[i], dst, b->m[i] + 1LL, b->m[i], b->k[i]};
+      eA[i] = dst;
+      elda[i] = b->m[i] + 1;
+    }
+    if ((ldb[i] & 1) && b->pitch_b[i] != SIZE_MAX) {
+      double* dst = reinterpret_cast<double*>(b->d_pitch + b->pitch_b[i]);
+      b->h_pc[n_pc++] = fmm::PitchCopy{B[i], ldb[i], dst, b->k[i] + 1LL, b->k[i], b->n[i]};
+      eB[i] = dst;
+      eldb[i] = b->k[i] + 1;
+    }
+  }
   int n_lc = 0;
   bool tma[2] = {true, true};
   for (int ph = 0; ph < 2; ++ph)
-    if (!b->jobs[ph].empty()) tma[ph] = batch_fill(b, ph, A, lda, B, ldb, C, ldc, &n_lc);
+    if (!b->jobs[ph].empty())
+      tma[ph] = batch_fill(b, ph, eA.data(), elda.data(), eB.data(), eldb.data(), C, ldc, &n_lc);
   for (int ph = 0; ph < 2; ++ph)
     if (!b->jobs[ph].empty())
       FMM_CUDA_TRY(cudaMemcpyAsync(b->d_jobs[ph], b->h_jobs[ph], sizeof(fmm::GemmArgs) * b->jobs[ph].size(),
                                    cudaMemcpyHostToDevice, st));
   if (n_lc > 0)
     FMM_CUDA_TRY(cudaMemcpyAsync(b->d_lc, b->h_lc, sizeof(fmm::LincombTask) * n_lc, cudaMemcpyHostToDevice, st));
+  if (n_pc > 0)
+    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_pc, b->h_pc, sizeof(fmm::PitchCopy) * n_pc, cudaMemcpyHostToDevice, st));
   if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventRecord(b->staged, st));
   if (b->n_tickets > 0) FMM_CUDA_TRY(cudaMemsetAsync(b->d_tickets, 0, sizeof(int) * b->n_tickets, st));
+  if (n_pc > 0) {
+    ProfScope pf(K_PITCH_COPY, st);
+    fmm::fmm_pitch_copy_kernel<<<dim3(256, (unsigned)n_pc), 256, 0, st>>>(b->d_pc);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    FMM_CUDA_TRY(cudaGetLastError());
+  }
   if (n_lc > 0) {
     ProfScope pf(K_LINCOMB_BATCH, st);
     fmm::fmm_lincomb_batch_kernel<<<dim3(64, (unsigned)b->max_slots, (unsigned)n_lc), 256, 0, st>>>(b->d_lc);

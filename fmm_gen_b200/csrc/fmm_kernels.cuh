@@ -1033,6 +1033,28 @@ __global__ void fmm_lincomb_batch_kernel(const LincombTask* tasks) {
   lincomb_body(tk.a, blockIdx.y);
 }
 
+// Column-major copies between pitches, many in one launch (task blockIdx.y): used to give
+// operands with an odd leading dimension the even pitch (16-byte column starts) that
+// tensor-memory-access staging needs.
+struct PitchCopy {
+  const double* src;
+  long long lds;
+  double* dst;
+  long long ldd;
+  int rows, cols;
+};
+
+__device__ __forceinline__ void pitch_copy_body(const PitchCopy& t) {
+  for (int j = blockIdx.x; j < t.cols; j += gridDim.x) {
+    const double* s = t.src + (long long)j * t.lds;
+    double* d = t.dst + (long long)j * t.ldd;
+    for (int i = threadIdx.x; i < t.rows; i += blockDim.x) d[i] = s[i];
+  }
+}
+
+__global__ void fmm_pitch_copy_kernel(const PitchCopy* tasks) { pitch_copy_body(tasks[blockIdx.y]); }
+__global__ void fmm_pitch_copy1_kernel(const PitchCopy t) { pitch_copy_body(t); }
+
 // M_Add: C_l += sum_r W[l, r] * M_r for every C block l, products applied in order r.
 struct ScatterArgs {
   double* C;

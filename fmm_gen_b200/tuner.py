@@ -1,0 +1,268 @@
+"""Per-problem algorithm selection for batches: a B200 performance model seeds the
+choice, batch-level measurements refine it.
+
+The reference ranks algorithms with an analytic model (meta/model_coefficient.py:36-100
+counts, per product, the nonzeros of U, V, W; meta/model_gen.py:65-102 turns them into
+time = actual_flops * tau + memops * alpha for its CPU blocking MC/KC/NC).  The same
+structure is re-derived here for this implementation on B200:
+
+  * compute: every product of a job is a sub-GEMM tiled 128 x 128 with k steps of 8.
+    A k step costs `kstep_s` on one SM at the plain kernel's rate; a product whose
+    operand sums are folded while staging costs `1 + fold_per_term * (T - 1)` times
+    that (T = the larger of its A and B term counts); pre-summed products cost 1.
+  * memory: the pre-sum pass reads every U/V term and writes each summed operand once
+    (HBM bytes / bandwidth, a separate pass), and the multi-destination epilogue reads
+    and writes one C tile per W nonzero, of which `c_exposed` is not hidden under the
+    MMAs.
+  * partition: the same fringe split as the library (algebra.partition); the strips
+    are classical jobs.
+Time is in the batch's throughput view: SM-seconds / SMs plus the exposed memory time
+(a batch keeps every SM busy, so wave quantisation of a single problem does not apply).
+
+The tuner takes the model's best candidate per problem, then measures the whole batch
+and re-assigns groups of problems (by the model's choice and margin) while that makes the
+measured batch faster.  The only tile shape of the FP64 kernel is 128 x 128; the other
+scheduling parameter, products per work unit, is chosen by the batch itself.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import algebra
+
+CANDIDATES: Tuple[str, ...] = ("classical", "222-1", "232-1", "333-1", "222-2")
+TILE = 128
+KSTEP = 8
+
+
+@dataclass
+class B200Model:
+    """Constants of the model; defaults are this implementation's measurements on B200
+    (plain FP64 kernel 34.5 TFLOP/s; folded 222-1 products at 1.7x a plain k step;
+    6.5 TB/s copy bandwidth)."""
+
+    sms: int = 148
+    plain_tflops: float = 34.5
+    hbm_gbs: float = 6500.0
+    fold_per_term: float = 0.7
+    c_exposed: float = 0.3
+    unit_overhead_s: float = 1.5e-6  # pipeline fill + epilogue latency per work unit
+
+    @property
+    def kstep_s(self) -> float:
+        per_sm = self.plain_tflops * 1e12 / self.sms
+        return 2.0 * TILE * TILE * KSTEP / per_sm
+
+
+def candidate_levels(name: str) -> Tuple[List[str], List[int]]:
+    algs, levels = [], []
+    for part in name.split("_"):
+        a, lv = part.split("-")
+        algs.append(a)
+        levels.append(int(lv))
+    return algs, levels
+
+
+_PLANS: Dict[str, algebra.FMMPlan] = {}
+
+
+def plan_of(name: str) -> Optional[algebra.FMMPlan]:
+    if name == "classical":
+        return None
+    if name not in _PLANS:
+        _PLANS[name] = algebra.make_plan(*candidate_levels(name))
+    return _PLANS[name]
+
+
+def model_counts(plan: algebra.FMMPlan) -> List[int]:
+    """[R, A additions, B additions, C updates]: the reference's comp_counter
+    (model_coefficient.py:36-100), from the composed U, V, W."""
+    nu = np.count_nonzero(plan.U, axis=0)
+    nv = np.count_nonzero(plan.V, axis=0)
+    return [plan.rank, int((nu - 1).sum()), int((nv - 1).sum()), int(np.count_nonzero(plan.W))]
+
+
+def _presummed(plan: algebra.FMMPlan, ms: int, ns: int, ks: int) -> bool:
+    """The library's rule for forming operand sums in HBM before the products."""
+    return plan.rank > 1 and ms * ns >= (1 << 20) and ks >= 256
+
+
+def _tiles(ms: int, ns: int) -> int:
+    return math.ceil(ms / TILE) * math.ceil(ns / TILE)
+
+
+def _classical_job(model: B200Model, m: int, n: int, k: int) -> Tuple[float, float, int]:
+    if m <= 0 or n <= 0 or k <= 0:
+        return 0.0, 0.0, 0
+    t = _tiles(m, n)
+    return t * math.ceil(k / KSTEP) * model.kstep_s, 0.0, t
+
+
+def job_costs(model: B200Model, name: str, m: int, n: int, k: int) -> Dict[str, float]:
+    """Modelled SM-seconds, exposed HBM seconds and work units of one problem."""
+    plan = plan_of(name)
+    if plan is None:
+        sm, mem, units = _classical_job(model, m, n, k)
+        return {"sm_s": sm, "mem_s": mem, "units": units}
+    p = algebra.partition(m, n, k, plan.dims)
+    sm = mem = 0.0
+    units = 0
+    if p.ms > 0 and p.ns > 0 and p.ks > 0:
+        tiles = _tiles(p.ms, p.ns)
+        ksteps = math.ceil(p.ks / KSTEP)
+        nu = np.count_nonzero(plan.U, axis=0)
+        nv = np.count_nonzero(plan.V, axis=0)
+        if _presummed(plan, p.ms, p.ns, p.ks):
+            factor = float(plan.rank)
+            na, nb = int((nu > 1).sum()), int((nv > 1).sum())
+            bytes_ = 8.0 * (nu[nu > 1].sum() * p.ms * p.ks + na * p.ms * p.ks +
+                            nv[nv > 1].sum() * p.ks * p.ns + nb * p.ks * p.ns)
+            mem += bytes_ / (model.hbm_gbs * 1e9)
+        else:
+            T = np.maximum(nu, nv)
+            factor = float((1.0 + model.fold_per_term * (T - 1)).sum())
+        sm += tiles * ksteps * model.kstep_s * factor
+        nnz_w = int(np.count_nonzero(plan.W))
+        mem += model.c_exposed * 16.0 * nnz_w * p.ms * p.ns / (model.hbm_gbs * 1e9)
+        units += tiles * max(1, min(plan.rank, math.ceil(plan.rank * ksteps / 512)))
+    for (mm, nn, kk) in ((p.md, p.nd, p.kr), (m, p.nr, k), (p.mr, p.nd, k)):
+        s2, _, u2 = _classical_job(model, mm, nn, kk)
+        sm += s2
+        units += u2
+    sm += units * model.unit_overhead_s
+    return {"sm_s": sm, "mem_s": mem, "units": units}
+
+
+def model_time(model: B200Model, name: str, m: int, n: int, k: int) -> float:
+    c = job_costs(model, name, m, n, k)
+    return c["sm_s"] / model.sms + c["mem_s"]
+
+
+def rank_candidates(model: B200Model, shape: Sequence[int],
+                    candidates: Sequence[str] = CANDIDATES) -> List[Tuple[str, float]]:
+    m, n, k = shape
+    return sorted(((c, model_time(model, c, m, n, k)) for c in candidates), key=lambda t: t[1])
+
+
+@dataclass
+class TuneReport:
+    choices: List[str]
+    model_choices: List[str]
+    trials: List[Tuple[str, float]] = field(default_factory=list)  # (description, measured ms)
+
+    def counts(self) -> Dict[str, int]:
+        out: Dict[str, int] = {}
+        for c in self.choices:
+            out[c] = out.get(c, 0) + 1
+        return out
+
+
+class BatchTuner:
+    """Chooses an algorithm per problem of a batch.
+
+    `measure(choices) -> milliseconds` times a whole batch with the given per-problem
+    algorithm names (the caller owns the operands; see `batch_timer`).  Without it the
+    model's choice is returned."""
+
+    def __init__(self, model: Optional[B200Model] = None, candidates: Sequence[str] = CANDIDATES):
+        self.model = model or B200Model()
+        self.candidates = tuple(candidates)
+
+    def model_choice(self, shapes: Sequence[Sequence[int]]) -> Tuple[List[str], List[List[Tuple[str, float]]]]:
+        ranked = [rank_candidates(self.model, s, self.candidates) for s in shapes]
+        return [r[0][0] for r in ranked], ranked
+
+    def tune(self, shapes: Sequence[Sequence[int]], measure=None, rounds: int = 2) -> TuneReport:
+        choices, ranked = self.model_choice(shapes)
+        rep = TuneReport(list(choices), list(choices))
+        if measure is None:
+            return rep
+        best = measure(choices)
+        rep.trials.append(("model choice", best))
+        for _ in range(rounds):
+            improved = False
+            # groups: problems the model gives to one FMM candidate; try each group on its
+            # runner-up, then on classical
+            for cand in self.candidates:
+                if cand == "classical":
+                    continue
+                idx = [i for i, c in enumerate(choices) if c == cand]
+                if not idx:
+                    continue
+                for alt_rank in (1, None):
+                    trial = list(choices)
+                    for i in idx:
+                        if alt_rank is None:
+                            trial[i] = "classical"
+                        else:
+                            trial[i] = ranked[i][alt_rank][0]
+                    if trial == choices:
+                        continue
+                    t = measure(trial)
+                    what = f"{cand} group ({len(idx)}) -> " + ("classical" if alt_rank is None else "runner-up")
+                    rep.trials.append((what, t))
+                    if t < best * 0.995:
+                        best, choices, improved = t, trial, True
+                        break
+            # problems the model sends to classical by a small margin: try their runner-up
+            close = [i for i, r in enumerate(ranked)
+                     if choices[i] == "classical" and len(r) > 1 and r[1][1] <= 1.05 * r[0][1]]
+            if close:
+                trial = list(choices)
+                for i in close:
+                    trial[i] = ranked[i][1][0] if ranked[i][0][0] == "classical" else ranked[i][0][0]
+                t = measure(trial)
+                rep.trials.append((f"near-tie classical ({len(close)}) -> FMM", t))
+                if t < best * 0.995:
+                    best, choices, improved = t, trial, True
+            if not improved:
+                break
+        rep.choices = list(choices)
+        return rep
+
+
+def random_batch_shapes(count: int = 512, lo: int = 256, hi: int = 4096, seed: int = 0) -> List[Tuple[int, int, int]]:
+    """m, n, k each round(exp(U(ln lo, ln hi))) from the seed (the batching workload)."""
+    rng = np.random.default_rng(seed)
+    d = np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), size=(count, 3)))).astype(int)
+    return [tuple(int(v) for v in row) for row in d]
+
+
+def batch_timer(runtime, shapes, As, Bs, Cs, reps: int = 3, warmup: int = 1):
+    """measure(choices) for BatchTuner: builds a Batch with the named plans and returns the
+    best of `reps` device-timed runs in milliseconds.  The runs add into Cs."""
+    import torch
+
+    plans: Dict[str, object] = {}
+
+    def plan(name):
+        if name == "classical":
+            return None
+        if name not in plans:
+            plans[name] = runtime.Plan.from_levels(*candidate_levels(name))
+        return plans[name]
+
+    def measure(choices: Sequence[str]) -> float:
+        b = runtime.Batch(shapes, [plan(c) for c in choices])
+        try:
+            for _ in range(warmup):
+                b.run(As, Bs, Cs)
+            times = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                b.run(As, Bs, Cs)
+                e1.record()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            return min(times)
+        finally:
+            torch.cuda.synchronize()
+            b.close()
+
+    measure.plans = plans
+    return measure
