@@ -298,6 +298,31 @@ def batch_512(rt, torch, dev, steps=3):
     return out
 
 
+def serving_2000(rt, torch, dev, window=1.0, rank=0, world=1):
+    """Continuous-batching request loop: Poisson arrivals at 2000 req/s for `window` s
+    (80% FP64 with m, n, k log-uniform in [256, 4096]; 10% FP64 rank-k 16000x16000x256;
+    10% split-BF16 222-2 8192^3), operands device-resident from admission, 160 GB HBM
+    budget; p50/p99 latency and effective TFLOPS over the window.  With N GPUs each rank
+    serves its deterministic share of the stream."""
+    from fmm_gen_b200 import serve
+
+    reqs = serve.poisson_requests(serve.Mix(rate=2000.0), window, seed=0)
+    if world > 1:
+        reqs = serve.shard_requests(reqs, world)[rank]
+    ex = serve.GpuExecutor(seed=0)
+    for kind in (serve.FP64, serve.SPLIT):  # first-use costs outside the window
+        ex.run_alone(next(r for r in reqs if r.kind == kind))
+    torch.cuda.empty_cache()
+    rep = serve.Server(ex, budget_bytes=160e9).run(reqs, window)
+    out = rep.summary()
+    out["arrivals"] = "Poisson 2000 req/s, seed 0" + (f", share of rank {rank}/{world}" if world > 1 else "")
+    out["budget_gb"] = 160
+    out["policy"] = "FIFO admission by HBM budget, bounded queue 4096; FP64 requests batched per launch"
+    del ex
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,6 +488,9 @@ def main():
         torch.cuda.empty_cache()
         extra["split_bf16_222_2_8192"] = split_bf16_8192(rt, torch, dev)
         extra["batch_512_fp64"] = batch_512(rt, torch, dev)
+        del A16, B16, C16
+        torch.cuda.empty_cache()
+        extra["serving_2000rps"] = serving_2000(rt, torch, dev, rank=rank, world=world)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

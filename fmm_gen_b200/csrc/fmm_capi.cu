@@ -1445,7 +1445,10 @@ void batch_free(fmm_batch* b) {
   delete b;
 }
 
-int batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
+// The host side of a batch: jobs per phase in scheduling order, unit ranges, and the sizes
+// of the tickets and workspaces.  Allocates no device memory (the plans' tables are
+// uploaded on first use by device_tables).
+int batch_build(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
   if (!out || count <= 0 || !m || !n || !k) return FMM_E_INVALID;
   for (int i = 0; i < count; ++i)
     if (m[i] < 0 || n[i] < 0 || k[i] < 0) return FMM_E_INVALID;
@@ -1501,15 +1504,6 @@ int batch_create(int count, const fmm_plan* const* plans, const int* m, const in
       return FMM_E_UNSUPPORTED;
     }
     b->unit_start[ph].push_back((int)acc);
-  }
-  auto fail = [&](cudaError_t e) {
-    batch_free(b);
-    return cuda_status(e);
-  };
-  cudaError_t e = cudaSuccess;
-  for (int ph = 0; ph < 2 && e == cudaSuccess; ++ph) {
-    const size_t nj = b->jobs[ph].size();
-    if (nj == 0) continue;
     for (auto& j : b->jobs[ph]) {
       DevTables* d = nullptr;
       rc = device_tables(j.plan, &d);
@@ -1518,6 +1512,23 @@ int batch_create(int count, const fmm_plan* const* plans, const int* m, const in
         return rc;
       }
     }
+  }
+  *out = b;
+  return FMM_OK;
+}
+
+int batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
+  fmm_batch* b = nullptr;
+  int rc = batch_build(count, plans, m, n, k, &b);
+  if (rc != FMM_OK) return rc;
+  auto fail = [&](cudaError_t e) {
+    batch_free(b);
+    return cuda_status(e);
+  };
+  cudaError_t e = cudaSuccess;
+  for (int ph = 0; ph < 2 && e == cudaSuccess; ++ph) {
+    const size_t nj = b->jobs[ph].size();
+    if (nj == 0) continue;
     e = cudaMalloc((void**)&b->d_jobs[ph], sizeof(fmm::GemmArgs) * nj);
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_start[ph], sizeof(int) * (nj + 1));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_jobs[ph], sizeof(fmm::GemmArgs) * nj);
@@ -1625,6 +1636,10 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
   return tma;
 }
 
+void batch_prepare(fmm_batch* b, const double* const* A, const long* lda, const double* const* B, const long* ldb,
+                   double* const* C, const long* ldc, int* n_lc_out, int* n_pc_out, bool tma[2]);
+int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool tma[2]);
+
 int batch_run(fmm_batch* b, const double* const* A, const long* lda, const double* const* B, const long* ldb,
               double* const* C, const long* ldc, cudaStream_t st) {
   if (!b || !A || !lda || !B || !ldb || !C || !ldc) return FMM_E_INVALID;
@@ -1641,6 +1656,25 @@ int batch_run(fmm_batch* b, const double* const* A, const long* lda, const doubl
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   FMM_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
   if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventSynchronize(b->staged));
+  int n_lc = 0, n_pc = 0;
+  bool tma[2] = {true, true};
+  batch_prepare(b, A, lda, B, ldb, C, ldc, &n_lc, &n_pc, tma);
+  for (int ph = 0; ph < 2; ++ph)
+    if (!b->jobs[ph].empty())
+      FMM_CUDA_TRY(cudaMemcpyAsync(b->d_jobs[ph], b->h_jobs[ph], sizeof(fmm::GemmArgs) * b->jobs[ph].size(),
+                                   cudaMemcpyHostToDevice, st));
+  if (n_lc > 0)
+    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_lc, b->h_lc, sizeof(fmm::LincombTask) * n_lc, cudaMemcpyHostToDevice, st));
+  if (n_pc > 0)
+    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_pc, b->h_pc, sizeof(fmm::PitchCopy) * n_pc, cudaMemcpyHostToDevice, st));
+  if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventRecord(b->staged, st));
+  return batch_launch(b, st, n_lc, n_pc, tma);
+}
+
+// This call's job tables (host staging): even-pitch copies for odd leading dimensions,
+// per-job arguments and tensor maps, pre-sum tasks.
+void batch_prepare(fmm_batch* b, const double* const* A, const long* lda, const double* const* B, const long* ldb,
+                   double* const* C, const long* ldc, int* n_lc_out, int* n_pc_out, bool tma[2]) {
   // Operands with an odd leading dimension and a reserved even-pitch copy are staged
   // through it (rows + 1 pitch); the others are used in place.
   std::vector<const double*> eA(A, A + b->count), eB(B, B + b->count);
@@ -1661,19 +1695,15 @@ int batch_run(fmm_batch* b, const double* const* A, const long* lda, const doubl
     }
   }
   int n_lc = 0;
-  bool tma[2] = {true, true};
   for (int ph = 0; ph < 2; ++ph)
     if (!b->jobs[ph].empty())
       tma[ph] = batch_fill(b, ph, eA.data(), elda.data(), eB.data(), eldb.data(), C, ldc, &n_lc);
-  for (int ph = 0; ph < 2; ++ph)
-    if (!b->jobs[ph].empty())
-      FMM_CUDA_TRY(cudaMemcpyAsync(b->d_jobs[ph], b->h_jobs[ph], sizeof(fmm::GemmArgs) * b->jobs[ph].size(),
-                                   cudaMemcpyHostToDevice, st));
-  if (n_lc > 0)
-    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_lc, b->h_lc, sizeof(fmm::LincombTask) * n_lc, cudaMemcpyHostToDevice, st));
-  if (n_pc > 0)
-    FMM_CUDA_TRY(cudaMemcpyAsync(b->d_pc, b->h_pc, sizeof(fmm::PitchCopy) * n_pc, cudaMemcpyHostToDevice, st));
-  if (cap == cudaStreamCaptureStatusNone) FMM_CUDA_TRY(cudaEventRecord(b->staged, st));
+  *n_lc_out = n_lc;
+  *n_pc_out = n_pc;
+}
+
+// Enqueue the launches of a prepared batch whose tables are (being) copied to the device.
+int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool tma[2]) {
   if (b->n_tickets > 0) FMM_CUDA_TRY(cudaMemsetAsync(b->d_tickets, 0, sizeof(int) * b->n_tickets, st));
   if (n_pc > 0) {
     ProfScope pf(K_PITCH_COPY, st);
@@ -1736,3 +1766,125 @@ int fmm_batch_destroy(fmm_batch* batch) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// One-shot batches for request loops: the batch is formed, run and released per call with
+// no cudaMalloc / cudaFree (those synchronise the device, which would stop the requests
+// of a serving loop from overlapping).  Device buffers come from the stream-ordered pool;
+// the job tables go through a ring of pinned host buffers, each reused only after the
+// copy out of it has completed.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct PinnedRing {
+  static constexpr int N = 8;
+  char* buf[N] = {};
+  size_t cap[N] = {};
+  cudaEvent_t ev[N] = {};
+  int next = 0;
+  std::mutex mu;
+};
+PinnedRing g_ring[kMaxDevices];
+
+int ring_acquire(int dev, size_t bytes, char** buf, cudaEvent_t* ev) {
+  PinnedRing& r = g_ring[dev];
+  std::lock_guard<std::mutex> lk(r.mu);
+  const int s = r.next;
+  r.next = (s + 1) % PinnedRing::N;
+  if (!r.ev[s]) FMM_CUDA_TRY(cudaEventCreateWithFlags(&r.ev[s], cudaEventDisableTiming));
+  FMM_CUDA_TRY(cudaEventSynchronize(r.ev[s]));  // the slot's previous copy is done
+  if (r.cap[s] < bytes) {
+    if (r.buf[s]) cudaFreeHost(r.buf[s]);
+    r.buf[s] = nullptr;
+    r.cap[s] = 0;
+    const size_t cap = std::max<size_t>(bytes + bytes / 2, (size_t)1 << 20);
+    FMM_CUDA_TRY(cudaMallocHost((void**)&r.buf[s], cap));
+    r.cap[s] = cap;
+  }
+  *buf = r.buf[s];
+  *ev = r.ev[s];
+  return FMM_OK;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int batch_submit(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k,
+                 const double* const* A, const long* lda, const double* const* B, const long* ldb, double* const* C,
+                 const long* ldc, cudaStream_t st) {
+  if (!A || !lda || !B || !ldb || !C || !ldc) return FMM_E_INVALID;
+  for (int i = 0; i < count; ++i) {
+    int rc = check_args(m[i], n[i], k[i], A[i], lda[i], B[i], ldb[i], C[i], ldc[i]);
+    if (rc != FMM_OK) return rc;
+  }
+  fmm_batch* b = nullptr;
+  int rc = batch_build(count, plans, m, n, k, &b);
+  if (rc != FMM_OK) return rc;
+  // table block (identical layout in pinned staging and on the device)
+  size_t off = 0, o_jobs[2], o_start[2];
+  for (int ph = 0; ph < 2; ++ph) {
+    off = align_up(off, 64);
+    o_jobs[ph] = off;
+    off += sizeof(fmm::GemmArgs) * b->jobs[ph].size();
+  }
+  for (int ph = 0; ph < 2; ++ph) {
+    off = align_up(off, 16);
+    o_start[ph] = off;
+    off += sizeof(int) * b->unit_start[ph].size();
+  }
+  off = align_up(off, 64);
+  const size_t o_lc = off;
+  off += sizeof(fmm::LincombTask) * b->n_lincomb;
+  off = align_up(off, 64);
+  const size_t o_pc = off;
+  off += sizeof(fmm::PitchCopy) * 2 * count;
+  const size_t table_bytes = align_up(off, 256);
+  const size_t o_tk = table_bytes;
+  const size_t o_ws = align_up(o_tk + sizeof(int) * b->n_tickets, 256);
+  const size_t o_pt = align_up(o_ws + b->ws_bytes, 256);
+  const size_t dev_bytes = o_pt + b->pitch_bytes;
+  char* stage = nullptr;
+  cudaEvent_t stage_ev = nullptr;
+  rc = ring_acquire(b->dev, table_bytes, &stage, &stage_ev);
+  char* blk = nullptr;
+  if (rc == FMM_OK) rc = cuda_status(cudaMallocAsync((void**)&blk, dev_bytes, st));
+  if (rc != FMM_OK) {
+    batch_free(b);
+    return rc;
+  }
+  for (int ph = 0; ph < 2; ++ph) {
+    b->h_jobs[ph] = reinterpret_cast<fmm::GemmArgs*>(stage + o_jobs[ph]);
+    b->d_jobs[ph] = reinterpret_cast<fmm::GemmArgs*>(blk + o_jobs[ph]);
+    b->d_start[ph] = reinterpret_cast<int*>(blk + o_start[ph]);
+    if (!b->unit_start[ph].empty())
+      std::memcpy(stage + o_start[ph], b->unit_start[ph].data(), sizeof(int) * b->unit_start[ph].size());
+  }
+  b->h_lc = reinterpret_cast<fmm::LincombTask*>(stage + o_lc);
+  b->d_lc = reinterpret_cast<fmm::LincombTask*>(blk + o_lc);
+  b->h_pc = reinterpret_cast<fmm::PitchCopy*>(stage + o_pc);
+  b->d_pc = reinterpret_cast<fmm::PitchCopy*>(blk + o_pc);
+  b->d_tickets = b->n_tickets ? reinterpret_cast<int*>(blk + o_tk) : nullptr;
+  b->d_ws = b->ws_bytes ? blk + o_ws : nullptr;
+  b->d_pitch = b->pitch_bytes ? blk + o_pt : nullptr;
+  int n_lc = 0, n_pc = 0;
+  bool tma[2] = {true, true};
+  batch_prepare(b, A, lda, B, ldb, C, ldc, &n_lc, &n_pc, tma);
+  rc = cuda_status(cudaMemcpyAsync(blk, stage, table_bytes, cudaMemcpyHostToDevice, st));
+  if (rc == FMM_OK) rc = cuda_status(cudaEventRecord(stage_ev, st));
+  if (rc == FMM_OK) rc = batch_launch(b, st, n_lc, n_pc, tma);
+  cudaError_t fe = cudaFreeAsync(blk, st);
+  if (rc == FMM_OK) rc = cuda_status(fe);
+  // the buffers belong to the pool and the ring: detach them before freeing the host side
+  for (int ph = 0; ph < 2; ++ph) b->h_jobs[ph] = nullptr, b->d_jobs[ph] = nullptr, b->d_start[ph] = nullptr;
+  b->h_lc = nullptr, b->d_lc = nullptr, b->h_pc = nullptr, b->d_pc = nullptr;
+  b->d_tickets = nullptr, b->d_ws = nullptr, b->d_pitch = nullptr;
+  batch_free(b);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int fmm_batch_submit(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k,
+                                const double* const* A, const long* lda, const double* const* B, const long* ldb,
+                                double* const* C, const long* ldc, void* stream) {
+  return batch_submit(count, plans, m, n, k, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+}

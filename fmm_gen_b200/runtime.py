@@ -96,6 +96,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_batch_units.restype = c_int
     lib.fmm_batch_destroy.argtypes = [c_void_p]
     lib.fmm_batch_destroy.restype = c_int
+    lib.fmm_batch_submit.argtypes = [c_int, ctypes.POINTER(c_void_p), c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p),
+                                     ctypes.POINTER(c_long), ctypes.POINTER(c_void_p), ctypes.POINTER(c_long),
+                                     ctypes.POINTER(c_void_p), ctypes.POINTER(c_long), c_void_p]
+    lib.fmm_batch_submit.restype = c_int
     for name in ("bl_dgemm", "bl_dgemm_strassen_abc", "bl_dgemm_strassen_ab", "bl_dgemm_strassen_naive"):
         f = getattr(lib, name)
         f.argtypes = [c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]
@@ -309,6 +313,31 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def batch_submit(plans, As, Bs, Cs, stream=None) -> None:
+    """One batch formed, run and released in a single stream-ordered call (no cudaMalloc /
+    cudaFree, so it does not synchronise the device): C_i += A_i @ B_i for every i, with
+    plans[i] a Plan or None (classical).  For request loops; results equal Batch.run's."""
+    import torch
+
+    count = len(As)
+    if not (len(Bs) == len(Cs) == len(plans) == count) or count == 0:
+        raise FmmError(-1, "plans and operand lists must have the same non-zero length")
+    lib = load_library()
+    ci, vp, cl = ctypes.c_int * count, ctypes.c_void_p * count, ctypes.c_long * count
+    ms, ns, ks, pa, pb, pc, la, lb, lc = [], [], [], [], [], [], [], [], []
+    for A, B, C in zip(As, Bs, Cs):
+        m, n, k = _check_operands(A, B, C)
+        ms.append(m); ns.append(n); ks.append(k)
+        pa.append(A.data_ptr()); la.append(_ld(A, m))
+        pb.append(B.data_ptr()); lb.append(_ld(B, k))
+        pc.append(C.data_ptr()); lc.append(_ld(C, m))
+    handles = vp(*[p.handle if p is not None else None for p in plans])
+    s = stream if stream is not None else torch.cuda.current_stream()
+    rc = lib.fmm_batch_submit(count, handles, ci(*ms), ci(*ns), ci(*ks), vp(*pa), cl(*la), vp(*pb), cl(*lb),
+                              vp(*pc), cl(*lc), ctypes.c_void_p(s.cuda_stream))
+    _check(rc, "fmm_batch_submit")
 
 
 # --------------------------------------------------------------------------------

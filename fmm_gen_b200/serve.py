@@ -1,0 +1,377 @@
+"""Serving: a continuous-batching request loop for mixed-shape, mixed-precision GEMMs.
+
+The reference has no serving layer (its entry point is one synchronous call per GEMM,
+meta/abc_gen_mix.py:448-472); this module is the loop that keeps a B200 busy with a stream
+of such calls:
+
+  * arrivals   - requests arrive on their own clock (a seeded Poisson stream in the
+                 benchmark); each is an FP64 C += A*B of some shape, or an FP32-accurate
+                 split-BF16 one.
+  * admission  - a request is admitted when its device bytes (operands plus workspace)
+                 fit in the HBM budget beside everything admitted and not yet finished;
+                 until then it waits in a bounded queue (arrivals beyond it are rejected).
+                 Admission brings its operands into device memory, where they stay until
+                 it finishes.
+  * batching   - every admitted FP64 request not yet dispatched joins the next FP64 batch:
+                 one persistent launch over all of their work units (fmm_batch_submit,
+                 per-request algorithm from the tuner's model).  Split-BF16 requests run on
+                 a second stream.  Up to `inflight` launches per stream are queued on the
+                 device, so requests that arrive while others run are admitted and
+                 dispatched as memory and launch slots free up, and their work overlaps.
+  * completion - an event per launch; when it completes, its requests' latencies are
+                 recorded and their memory returns to the budget.
+
+Results do not depend on the mix: a batch gives each problem exactly the arithmetic of a
+single call with the same algorithm, and the algorithm depends on the shape only.
+
+The executor is pluggable: GpuExecutor runs on the device through the library;
+tests drive the same loop with a simulated executor on the CPU.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import tuner
+
+FP64, SPLIT = "fp64", "split"
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str                      # FP64 or SPLIT
+    shape: Tuple[int, int, int]    # (m, n, k)
+    algorithm: str                 # tuner candidate name ("classical", "222-1", ...)
+    arrival: float                 # seconds from the start of the run
+    admitted: Optional[float] = None
+    dispatched: Optional[float] = None
+    done: Optional[float] = None
+    nbytes: int = 0
+    handle: object = None          # executor state (operands)
+
+    @property
+    def flops(self) -> float:
+        m, n, k = self.shape
+        return 2.0 * m * n * k
+
+    @property
+    def latency(self) -> Optional[float]:
+        return None if self.done is None else self.done - self.arrival
+
+
+def request_bytes(kind: str, shape: Sequence[int], algorithm: str) -> int:
+    """Device bytes a request holds while admitted: operands, C and workspaces."""
+    m, n, k = shape
+    if kind == SPLIT:
+        plan = tuner.plan_of(algorithm)
+        R = plan.rank if plan is not None else 1
+        dims = plan.dims if plan is not None else (1, 1, 1)
+        ms, ks, ns = m // dims[0], k // dims[1], n // dims[2]
+        kpad = -(-ks // 64) * 64
+        return 4 * (m * k + k * n) + 8 * m * n + 6 * R * (ms + ns) * kpad
+    ws = 0
+    plan = tuner.plan_of(algorithm)
+    if plan is not None:
+        p = tuner.algebra.partition(m, n, k, plan.dims)
+        if tuner._presummed(plan, p.ms, p.ns, p.ks):
+            nu = np.count_nonzero(plan.U, axis=0)
+            nv = np.count_nonzero(plan.V, axis=0)
+            ws = 8 * (int((nu > 1).sum()) * p.ms * p.ks + int((nv > 1).sum()) * (p.ks + 1) * p.ns)
+    pitch = 8 * ((m + 1) * k if m & 1 else 0) + 8 * ((k + 1) * n if k & 1 else 0)
+    return 8 * (m * k + k * n + m * n) + ws + pitch
+
+
+@dataclass
+class Mix:
+    """The offered load: Poisson arrivals at `rate` per second; a fraction `f_rank_k` of
+    rank-k FP64 requests, `f_split` of split-BF16 ones, the rest FP64 with m, n, k each
+    log-uniform in [lo, hi]."""
+
+    rate: float = 2000.0
+    f_rank_k: float = 0.10
+    f_split: float = 0.10
+    lo: int = 256
+    hi: int = 4096
+    rank_k_shape: Tuple[int, int, int] = (16000, 16000, 256)
+    split_shape: Tuple[int, int, int] = (8192, 8192, 8192)
+    split_algorithm: str = "222-2"
+
+
+def poisson_requests(mix: Mix, window: float, seed: int = 0,
+                     model: Optional[tuner.B200Model] = None) -> List[Request]:
+    rng = np.random.default_rng(seed)
+    model = model or tuner.B200Model()
+    out: List[Request] = []
+    t, rid = 0.0, 0
+    cache: Dict[Tuple[int, int, int], str] = {}
+    while True:
+        t += rng.exponential(1.0 / mix.rate)
+        if t >= window:
+            break
+        u = rng.random()
+        if u < mix.f_split:
+            kind, shape, alg = SPLIT, mix.split_shape, mix.split_algorithm
+        else:
+            kind = FP64
+            if u < mix.f_split + mix.f_rank_k:
+                shape = mix.rank_k_shape
+            else:
+                d = np.rint(np.exp(rng.uniform(math.log(mix.lo), math.log(mix.hi), size=3))).astype(int)
+                shape = (int(d[0]), int(d[1]), int(d[2]))
+            if shape not in cache:
+                cache[shape] = tuner.rank_candidates(model, shape)[0][0]
+            alg = cache[shape]
+        out.append(Request(rid, kind, shape, alg, t, nbytes=request_bytes(kind, shape, alg)))
+        rid += 1
+    return out
+
+
+class Launch:
+    """Requests dispatched together, and how to tell that they finished."""
+
+    def __init__(self, kind: str, reqs: List[Request], token):
+        self.kind, self.reqs, self.token = kind, reqs, token
+
+
+@dataclass
+class Report:
+    window: float
+    offered: int
+    completed: int
+    rejected: int
+    backlog: int                  # arrived in the window, not finished at its end
+    latencies: List[float] = field(default_factory=list)
+    flops_done: float = 0.0
+    by_kind: Dict[str, Dict[str, float]] = field(default_factory=dict)
+    launches: Dict[str, int] = field(default_factory=dict)
+    peak_bytes: int = 0
+
+    def percentile(self, q: float) -> Optional[float]:
+        return float(np.percentile(self.latencies, q)) if self.latencies else None
+
+    def summary(self) -> Dict[str, object]:
+        return {
+            "window_s": self.window, "offered": self.offered, "completed": self.completed,
+            "rejected": self.rejected, "backlog_at_end": self.backlog,
+            "p50_ms": None if not self.latencies else 1e3 * self.percentile(50),
+            "p99_ms": None if not self.latencies else 1e3 * self.percentile(99),
+            "tflops_effective": self.flops_done / self.window / 1e12,
+            "by_kind": self.by_kind, "launches": self.launches, "peak_admitted_gb": self.peak_bytes / 1e9,
+        }
+
+
+class Server:
+    """The request loop.  `executor` provides admit(req) (bring operands to the device),
+    launch(kind, reqs) -> token, done(token) -> bool, release(req) and sync()."""
+
+    def __init__(self, executor, budget_bytes: float = 160e9, max_queue: int = 4096, max_batch: int = 512,
+                 inflight: int = 2, clock: Callable[[], float] = time.perf_counter,
+                 sleep: Callable[[float], None] = time.sleep):
+        self.ex = executor
+        self.budget = budget_bytes
+        self.max_queue = max_queue
+        self.max_batch = max_batch
+        self.inflight = inflight
+        self.clock = clock
+        self.sleep = sleep
+
+    def run(self, requests: Sequence[Request], window: float, drain: bool = True) -> Report:
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        queue: deque = deque()
+        ready: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
+        running: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
+        in_use = peak = 0
+        rejected = 0
+        nxt = 0
+        launches = {FP64: 0, SPLIT: 0}
+        t0 = self.clock()
+        now = 0.0
+        while True:
+            now = self.clock() - t0
+            open_ = now < window
+            if open_:
+                # arrivals up to now
+                while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                    if len(queue) >= self.max_queue or reqs[nxt].nbytes > self.budget:
+                        rejected += 1
+                    else:
+                        queue.append(reqs[nxt])
+                    nxt += 1
+                # admission in arrival order while memory allows
+                while queue and in_use + queue[0].nbytes <= self.budget:
+                    r = queue.popleft()
+                    self.ex.admit(r)
+                    r.admitted = self.clock() - t0
+                    in_use += r.nbytes
+                    peak = max(peak, in_use)
+                    ready[r.kind].append(r)
+            # dispatch: all ready FP64 requests form one batch; split requests one by one
+            for kind in (FP64, SPLIT):
+                while ready[kind] and len(running[kind]) < self.inflight:
+                    take = self.max_batch if kind == FP64 else 1
+                    group = [ready[kind].popleft() for _ in range(min(take, len(ready[kind])))]
+                    tnow = self.clock() - t0
+                    for r in group:
+                        r.dispatched = tnow
+                    running[kind].append(Launch(kind, group, self.ex.launch(kind, group)))
+                    launches[kind] += 1
+            # completions (launches on one stream finish in order)
+            progressed = False
+            for kind in (FP64, SPLIT):
+                while running[kind] and self.ex.done(running[kind][0].token):
+                    lch = running[kind].popleft()
+                    tdone = self.clock() - t0
+                    for r in lch.reqs:
+                        r.done = tdone
+                        self.ex.release(r)
+                        in_use -= r.nbytes
+                    progressed = True
+            busy = any(running.values()) or any(ready.values())
+            if not open_ and (not drain or not busy):
+                break  # what still waits in the queue is the backlog
+            if nxt == len(reqs) and not queue and not busy:
+                break  # every request has arrived and finished
+            if progressed:
+                continue
+            if not busy and not queue and open_:
+                nxt_t = reqs[nxt].arrival if nxt < len(reqs) else window
+                self.sleep(min(max(0.0, min(nxt_t, window) - now), 1e-3))
+            else:
+                self.sleep(2e-5)
+        self.ex.sync()
+        arrived = [r for r in reqs if r.arrival < window]
+        done_in = [r for r in arrived if r.done is not None and r.done <= window]
+        rep = Report(window=window, offered=len(arrived), completed=len(done_in), rejected=rejected,
+                     backlog=sum(1 for r in arrived if r.done is None or r.done > window) - rejected,
+                     latencies=[r.latency for r in done_in], flops_done=sum(r.flops for r in done_in),
+                     launches=launches, peak_bytes=peak)
+        for kind in (FP64, SPLIT):
+            ks = [r for r in done_in if r.kind == kind]
+            if ks:
+                lat = [r.latency for r in ks]
+                rep.by_kind[kind] = {"completed": len(ks), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                                     "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                                     "tflops_effective": sum(r.flops for r in ks) / window / 1e12}
+        return rep
+
+
+class GpuExecutor:
+    """Runs requests on the current CUDA device through the library.  Operands are made on
+    the device from a per-request seed (A, B ~ U(-1,1) for FP64; A ~ N(0,1), B log-uniform
+    2^-10..2^10 with random sign for split-BF16; C = 0), so a request can be re-run alone
+    with the same inputs; keep=True keeps every result for such comparisons."""
+
+    def __init__(self, seed: int = 0, keep: bool = False):
+        import torch
+
+        from . import runtime as rt
+
+        self.torch, self.rt = torch, rt
+        self.seed, self.keep = seed, keep
+        self.streams = {FP64: torch.cuda.Stream(), SPLIT: torch.cuda.Stream()}
+        self.plans: Dict[str, object] = {}
+        self.results: Dict[int, object] = {}
+
+    def plan(self, name: str):
+        if name == "classical":
+            return None
+        if name not in self.plans:
+            self.plans[name] = self.rt.Plan.from_levels(*tuner.candidate_levels(name))
+        return self.plans[name]
+
+    def operands(self, r: Request):
+        torch, rt = self.torch, self.rt
+        m, n, k = r.shape
+        g = torch.Generator(device="cuda").manual_seed(self.seed * 1000003 + r.rid)
+        if r.kind == FP64:
+            A = rt.colmajor(m, k, device="cuda").uniform_(-1, 1, generator=g)
+            B = rt.colmajor(k, n, device="cuda").uniform_(-1, 1, generator=g)
+        else:
+            A = rt.colmajor(m, k, dtype=torch.float32, device="cuda").normal_(generator=g)
+            e = torch.empty((k, n), device="cuda").uniform_(-10, 10, generator=g)
+            s = torch.empty((k, n), device="cuda").uniform_(-1, 1, generator=g).sign()
+            B = rt.colmajor(k, n, dtype=torch.float32, device="cuda").copy_(s * torch.exp2(e))
+            del e, s
+        C = rt.colmajor(m, n, device="cuda").zero_()
+        return A, B, C
+
+    def admit(self, r: Request) -> None:
+        with self.torch.cuda.stream(self.streams[r.kind]):
+            r.handle = self.operands(r)
+
+    def launch(self, kind: str, reqs: List[Request]):
+        torch, rt = self.torch, self.rt
+        st = self.streams[kind]
+        with torch.cuda.stream(st):
+            if kind == FP64:
+                rt.batch_submit([self.plan(r.algorithm) for r in reqs], [r.handle[0] for r in reqs],
+                                [r.handle[1] for r in reqs], [r.handle[2] for r in reqs], stream=st)
+            else:
+                for r in reqs:
+                    rt.split_gemm(self.plan(r.algorithm), *r.handle, stream=st)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        return ev
+
+    def done(self, token) -> bool:
+        return token.query()
+
+    def release(self, r: Request) -> None:
+        if self.keep:
+            self.results[r.rid] = r.handle[2].cpu()
+        r.handle = None
+
+    def sync(self) -> None:
+        self.torch.cuda.synchronize()
+
+    def run_alone(self, r: Request):
+        """The request by itself (same inputs, same algorithm), for comparison."""
+        A, B, C = self.operands(r)
+        if r.kind == FP64:
+            p = self.plan(r.algorithm)
+            if p is None:
+                self.rt.plain_gemm(A, B, C)
+            else:
+                self.rt.fmm_gemm(p, A, B, C, "abc")
+        else:
+            self.rt.split_gemm(self.plan(r.algorithm), A, B, C)
+        self.torch.cuda.synchronize()
+        return C.cpu()
+
+
+def shard_requests(requests: Sequence[Request], world: int, model: Optional[tuner.B200Model] = None) -> List[List[Request]]:
+    """Requests to GPUs for a multi-GPU server: in arrival order, each request goes to the
+    GPU with the least modelled outstanding work (work drains at one GPU-second per second;
+    among idle GPUs, the one given the least work so far), the same deterministic answer
+    on every rank without any exchange."""
+    model = model or tuner.B200Model()
+    load = [0.0] * world   # modelled work still queued on each GPU
+    total = [0.0] * world  # work given to each GPU so far (breaks ties between idle GPUs)
+    last = 0.0
+    out: List[List[Request]] = [[] for _ in range(world)]
+    for r in sorted(requests, key=lambda q: q.arrival):
+        dt = r.arrival - last
+        last = r.arrival
+        load = [max(0.0, x - dt) for x in load]
+        cost = model_cost(model, r)
+        g = min(range(world), key=lambda i: (load[i], total[i], i))
+        load[g] += cost
+        total[g] += cost
+        out[g].append(r)
+    return out
+
+
+def model_cost(model: tuner.B200Model, r: Request) -> float:
+    m, n, k = r.shape
+    if r.kind == SPLIT:
+        # bf16 plane products at about half the measured dense bf16 rate, six per product
+        plan = tuner.plan_of(r.algorithm)
+        frac = plan.rank / float(np.prod(plan.dims)) if plan is not None else 1.0
+        return 6 * frac * r.flops / 0.8e15
+    return tuner.model_time(model, r.algorithm, m, n, k)

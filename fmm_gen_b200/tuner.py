@@ -266,3 +266,20 @@ def batch_timer(runtime, shapes, As, Bs, Cs, reps: int = 3, warmup: int = 1):
 
     measure.plans = plans
     return measure
+
+
+def shard_problems(shapes: Sequence[Sequence[int]], choices: Sequence[str], world: int,
+                   model: Optional[B200Model] = None) -> List[List[int]]:
+    """Independent problems to GPUs: longest modelled problem first, each to the GPU with
+    the least modelled work so far (LPT).  Deterministic, so every rank computes the same
+    assignment without an exchange; returns the problem indices per rank."""
+    model = model or B200Model()
+    cost = [model_time(model, c, *s) for s, c in zip(shapes, choices)]
+    order = sorted(range(len(shapes)), key=lambda i: (-cost[i], i))
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        g = min(range(world), key=lambda r: (load[r], r))
+        load[g] += cost[i]
+        out[g].append(i)
+    return [sorted(x) for x in out]

@@ -155,6 +155,17 @@ int fmm_batch_create(int count, const fmm_plan *const *plans, const int *m, cons
                      fmm_batch **out);
 int fmm_batch_dgemm(fmm_batch *batch, const double *const *A, const long *lda, const double *const *B,
                     const long *ldb, double *const *C, const long *ldc, void *stream);
+/* A batch formed, run and released in one stream-ordered call, for request loops that
+ * form a new batch at every step: no cudaMalloc or cudaFree (both synchronise the
+ * device, which would stop requests already on the GPU from overlapping with the next
+ * batch).  Device buffers come from the stream-ordered pool; the job tables are staged
+ * through a ring of 8 pinned host buffers owned by the library, each reused only after
+ * the copy out of it has completed (so at most 8 calls' copies are pending).  Same
+ * results as fmm_batch_create + fmm_batch_dgemm; not meant for stream capture. */
+int fmm_batch_submit(int count, const fmm_plan *const *plans, const int *m, const int *n, const int *k,
+                     const double *const *A, const long *lda, const double *const *B, const long *ldb,
+                     double *const *C, const long *ldc, void *stream);
+
 /* Work units of the main launch (phase 0) or of the k-fringe launch (phase 1). */
 int fmm_batch_units(const fmm_batch *batch, int phase);
 int fmm_batch_destroy(fmm_batch *batch);

@@ -1,0 +1,122 @@
+"""The serving loop's scheduling on the CPU: a simulated executor whose launches take
+their modelled time on a simulated clock, so admission, batching, overlap and the
+window accounting are checked exactly and quickly.  (GPU runs: tests/test_gpu_serve.py.)"""
+import numpy as np
+import pytest
+
+from fmm_gen_b200 import serve, tuner
+
+
+class SimClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-6)
+
+
+class SimExecutor:
+    """One simulated GPU: launches (from either stream) run back to back, each taking the
+    modelled time of its requests (a batch: the sum, as one persistent launch shares the
+    SMs among them)."""
+
+    def __init__(self, clock, speed=1.0):
+        self.clock, self.speed = clock, speed
+        self.gpu_free = 0.0
+        self.admitted, self.released, self.batches = [], [], []
+        self.model = tuner.B200Model()
+
+    def admit(self, r):
+        self.admitted.append(r.rid)
+
+    def launch(self, kind, reqs):
+        cost = sum(serve.model_cost(self.model, r) for r in reqs) / self.speed
+        start = max(self.clock(), self.gpu_free)
+        self.gpu_free = start + cost
+        self.batches.append((kind, [r.rid for r in reqs]))
+        return start + cost
+
+    def done(self, token):
+        return self.clock() >= token
+
+    def release(self, r):
+        self.released.append(r.rid)
+
+    def sync(self):
+        pass
+
+
+def run(reqs, window, **kw):
+    clk = SimClock()
+    ex = SimExecutor(clk, kw.pop("speed", 1.0))
+    srv = serve.Server(ex, clock=clk, sleep=clk.sleep, **kw)
+    return srv.run(reqs, window), ex
+
+
+def test_poisson_stream_is_seeded_and_has_the_mix():
+    mix = serve.Mix(rate=2000.0)
+    a = serve.poisson_requests(mix, 1.0, seed=3)
+    b = serve.poisson_requests(mix, 1.0, seed=3)
+    assert [(r.shape, r.arrival) for r in a] == [(r.shape, r.arrival) for r in b]
+    assert 1800 < len(a) < 2200
+    kinds = [r.kind for r in a]
+    assert abs(kinds.count(serve.SPLIT) / len(a) - 0.10) < 0.03
+    rk = sum(1 for r in a if r.shape == (16000, 16000, 256))
+    assert abs(rk / len(a) - 0.10) < 0.03
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) > 0)
+
+
+def test_light_load_serves_everything_with_service_time_latency():
+    mix = serve.Mix(rate=50.0, f_rank_k=0.0, f_split=0.0, lo=256, hi=512)
+    reqs = serve.poisson_requests(mix, 0.5, seed=1)
+    rep, ex = run(reqs, 0.5)
+    assert rep.completed + rep.backlog == rep.offered and rep.rejected == 0
+    assert rep.completed >= rep.offered - 2
+    assert max(rep.latencies) < 0.01      # no queueing at 50 req/s of small GEMMs
+    assert sorted(ex.released) == sorted(ex.admitted)
+
+
+def test_requests_arriving_during_a_launch_join_the_next_batch():
+    mix = serve.Mix(rate=4000.0, f_rank_k=0.0, f_split=0.0, lo=1024, hi=2048)
+    reqs = serve.poisson_requests(mix, 0.05, seed=2)
+    rep, ex = run(reqs, 0.05, inflight=1)
+    fp = [ids for kind, ids in ex.batches if kind == serve.FP64]
+    assert len(fp) < len(reqs) and max(len(ids) for ids in fp) > 1
+    # batches are formed in arrival order
+    flat = [i for ids in fp for i in ids]
+    assert flat == sorted(flat)
+
+
+def test_admission_respects_the_budget_and_the_queue_bounds_overload():
+    mix = serve.Mix(rate=2000.0)
+    reqs = serve.poisson_requests(mix, 0.2, seed=4)
+    budget = 20e9
+    rep, ex = run(reqs, 0.2, budget_bytes=budget, max_queue=64)
+    assert rep.peak_bytes <= budget
+    assert rep.rejected > 0                      # overload: the bounded queue sheds
+    assert rep.backlog > 0
+    assert rep.completed + rep.backlog + rep.rejected == rep.offered
+    assert all(r.done is None or r.done >= r.arrival for r in reqs)
+
+
+def test_split_and_fp64_streams_overlap():
+    mix = serve.Mix(rate=400.0, f_rank_k=0.0, f_split=0.5, lo=256, hi=1024)
+    reqs = serve.poisson_requests(mix, 0.1, seed=5)
+    rep, ex = run(reqs, 0.1)
+    assert {k for k, _ in ex.batches} == {serve.FP64, serve.SPLIT}
+    assert rep.by_kind[serve.FP64]["p50_ms"] < rep.by_kind[serve.SPLIT]["p50_ms"]
+
+
+def test_sharding_is_deterministic_and_balanced():
+    reqs = serve.poisson_requests(serve.Mix(rate=2000.0), 0.5, seed=6)
+    a = serve.shard_requests(reqs, 4)
+    b = serve.shard_requests(reqs, 4)
+    assert [[r.rid for r in s] for s in a] == [[r.rid for r in s] for s in b]
+    assert sorted(r.rid for s in a for r in s) == [r.rid for r in reqs]
+    model = tuner.B200Model()
+    work = [sum(serve.model_cost(model, r) for r in s) for s in a]
+    assert max(work) / min(work) < 1.3
