@@ -345,14 +345,14 @@ bool make_tensor_map(CUtensorMap* map, const double* base, long long rows, long 
   return r == CUDA_SUCCESS;
 }
 
-// Products per tile are split into chunks when there are too few tile positions to fill
-// the persistent grid several times over.
+// Work units take one product each (product-major order): the CTAs running at one time
+// then work on one or two products, whose operand panels stay in L2, and the per-tile
+// tickets keep the C updates in product order.  Measured on B200 against units of many
+// products: 16384^3 222-1 x 333-1 35.6 -> 36.5 TFLOP/s, 222-2 41.0 -> 41.3.
 int choose_chunks(int ntiles, int nprod, int nsm) {
-  const long long want = 16LL * nsm;
-  long long c = (want + ntiles - 1) / ntiles;
-  if (c < 1) c = 1;
-  if (c > nprod) c = nprod;
-  return (int)c;
+  (void)ntiles;
+  (void)nsm;
+  return nprod;
 }
 
 // Launch the persistent DMMA GEMM over sub-blocks of size ms x ks x ns.
@@ -463,6 +463,13 @@ int grid_for(long long total, int threads) {
   return (int)b;
 }
 
+// Blocks along the element dimension of fmm_lincomb_kernel (each covers LINCOMB_CHUNK
+// row pairs; beyond the grid limit the blocks loop).
+unsigned lincomb_chunks(long long pairs) {
+  const long long c = (pairs + fmm::LINCOMB_CHUNK - 1) / fmm::LINCOMB_CHUNK;
+  return (unsigned)std::max<long long>(1, std::min<long long>(c, 65535));
+}
+
 // Fringe GEMMs, same regions and order as the reference's dynamic peeling.
 int peel(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, double* C,
          long long ldc, int dim1, int dim2, int dim3, cudaStream_t st) {
@@ -508,7 +515,7 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     la.terms = d.terms;
     la.plist = d.plistA;
     la.side = 0;
-    const dim3 g((unsigned)grid_for((long long)(ms + 1) / 2 * ks, 256), (unsigned)ps.nslotA);
+    const dim3 g((unsigned)ps.nslotA, lincomb_chunks((long long)(ms + 1) / 2 * ks));
     ProfScope pf(K_LINCOMB, st);
     fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(la);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -528,7 +535,7 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     lb.terms = d.terms;
     lb.plist = d.plistB;
     lb.side = 1;
-    const dim3 g((unsigned)grid_for((long long)(ks + 1) / 2 * ns, 256), (unsigned)ps.nslotB);
+    const dim3 g((unsigned)ps.nslotB, lincomb_chunks((long long)(ks + 1) / 2 * ns));
     ProfScope pf(K_LINCOMB, st);
     fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(lb);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -619,7 +626,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         la.terms = d->terms;
         la.side = 0;
         la.plist = nullptr;
-        const dim3 ga((unsigned)grid_for((long long)ms * ks, 256), (unsigned)R);
+        const dim3 ga((unsigned)R, lincomb_chunks((long long)(ms + 1) / 2 * ks));
         {
           ProfScope ps(K_LINCOMB, st);
           fmm::fmm_lincomb_kernel<<<ga, 256, 0, st>>>(la);
@@ -636,7 +643,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         lb.ldo = ks;
         lb.out_stride = (long long)ks * ns;
         lb.side = 1;
-        const dim3 gb((unsigned)grid_for((long long)ks * ns, 256), (unsigned)R);
+        const dim3 gb((unsigned)R, lincomb_chunks((long long)(ks + 1) / 2 * ns));
         {
           ProfScope ps(K_LINCOMB, st);
           fmm::fmm_lincomb_kernel<<<gb, 256, 0, st>>>(lb);
@@ -1343,6 +1350,7 @@ struct fmm_batch {
   std::vector<Job> jobs[2];        // phase 0: FMM cores and disjoint strips; phase 1: k strips
   std::vector<int> unit_start[2];
   int max_slots = 0;
+  unsigned max_lincomb_chunks = 1;
   int n_lincomb = 0;
   size_t n_tickets = 0, ws_bytes = 0;
   fmm::GemmArgs* d_jobs[2] = {nullptr, nullptr};
@@ -1416,6 +1424,8 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
     b->ws_bytes += sizeof(double) * ((size_t)ms * ks * j.nA + (size_t)j.ldT * ns * j.nB);
     b->ws_bytes = (b->ws_bytes + 255) & ~(size_t)255;
     b->max_slots = std::max(b->max_slots, std::max(j.nA, j.nB));
+    b->max_lincomb_chunks = std::max({b->max_lincomb_chunks, lincomb_chunks((long long)(ms + 1) / 2 * ks),
+                                      lincomb_chunks((long long)(ks + 1) / 2 * ns)});
     b->n_lincomb += (j.nA > 0) + (j.nB > 0);
   }
   j.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
@@ -1713,7 +1723,8 @@ int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool t
   }
   if (n_lc > 0) {
     ProfScope pf(K_LINCOMB_BATCH, st);
-    fmm::fmm_lincomb_batch_kernel<<<dim3(64, (unsigned)b->max_slots, (unsigned)n_lc), 256, 0, st>>>(b->d_lc);
+    fmm::fmm_lincomb_batch_kernel<<<dim3((unsigned)b->max_slots, b->max_lincomb_chunks, (unsigned)n_lc), 256, 0, st>>>(
+        b->d_lc);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     FMM_CUDA_TRY(cudaGetLastError());
   }

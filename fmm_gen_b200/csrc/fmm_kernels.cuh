@@ -80,6 +80,7 @@ constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_S
 constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
 constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
 constexpr int C_PREFETCH_STEPS = 24;  // k steps before a product's end at which its C tiles are prefetched
+                                      // (at its first k step when it has fewer)
 constexpr int PROD_REGS = 72;
 constexpr int CONS_REGS = 184;
 static_assert(NPROD * PROD_REGS + NCONS * CONS_REGS <= NTHREADS * LAUNCH_REGS,
@@ -874,7 +875,7 @@ __device__ __forceinline__ void consumer(const Src& src, const double* stages, u
         const double* opA = stages + (size_t)stage * STAGE_SZ;
         const double* opB = opA + OPA_SZ;
         mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), src.status());
-        if (s == nks - C_PREFETCH_STEPS) prefetch_c_tiles(a, p, w.m0, w.n0, ct);
+        if (s == (nks > C_PREFETCH_STEPS ? nks - C_PREFETCH_STEPS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, ct);
         mma_stage(opA, opB, acc, wm, wn, g, t4);
         // The stage is refilled by TMA as soon as every warp has arrived; the fence
         // makes this warp's shared-memory fragment loads complete before its arrival
@@ -978,16 +979,25 @@ struct LincombArgs {
   int side;
 };
 
-__device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j) {
+// Elements per block: output j = blockIdx.x varies fastest in the grid, so the blocks
+// resident at one time cover the same element range for many outputs and read each input
+// element from HBM about once (the other reads hit L2).
+constexpr int LINCOMB_CHUNK = 256 * 16;  // row pairs per block
+
+__device__ __forceinline__ long long lincomb_pairs(const LincombArgs& a) {
+  return (long long)((a.rows + 1) / 2) * a.cols;
+}
+
+__device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j, long long chunk) {
   const int r = a.plist ? a.plist[j] : j;
   const Prod p = a.prods[r];
   const int t0 = a.side == 0 ? p.a0 : p.b0;
   const int nt = a.side == 0 ? p.na : p.nb;
   double* out = a.out + (long long)j * a.out_stride;
   const int hr = (a.rows + 1) / 2;  // row pairs per column
-  const long long total = (long long)hr * a.cols;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
+  const long long total = lincomb_pairs(a);
+  const long long e1 = min(total, (chunk + 1) * LINCOMB_CHUNK);
+  for (long long e = chunk * LINCOMB_CHUNK + threadIdx.x; e < e1; e += blockDim.x) {
     const int i = 2 * (int)(e % hr);
     const long long c = e / hr;
     const bool two = i + 1 < a.rows;
@@ -1017,10 +1027,13 @@ __device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j) {
   }
 }
 
-__global__ void fmm_lincomb_kernel(const LincombArgs a) { lincomb_body(a, blockIdx.y); }
+__global__ void fmm_lincomb_kernel(const LincombArgs a) {
+  const long long nchunk = (lincomb_pairs(a) + LINCOMB_CHUNK - 1) / LINCOMB_CHUNK;
+  for (long long c = blockIdx.y; c < nchunk; c += gridDim.y) lincomb_body(a, blockIdx.x, c);
+}
 
-// The operand sums of many problems in one launch: task blockIdx.z, output blockIdx.y
-// (tasks with fewer outputs return at once), elements grid-strided over blockIdx.x.
+// The operand sums of many problems in one launch: task blockIdx.z, output blockIdx.x
+// (tasks with fewer outputs return at once), element chunks over blockIdx.y.
 struct LincombTask {
   LincombArgs a;
   int nout;
@@ -1029,8 +1042,9 @@ struct LincombTask {
 
 __global__ void fmm_lincomb_batch_kernel(const LincombTask* tasks) {
   const LincombTask& tk = tasks[blockIdx.z];
-  if ((int)blockIdx.y >= tk.nout) return;
-  lincomb_body(tk.a, blockIdx.y);
+  if ((int)blockIdx.x >= tk.nout) return;
+  const long long nchunk = (lincomb_pairs(tk.a) + LINCOMB_CHUNK - 1) / LINCOMB_CHUNK;
+  for (long long c = blockIdx.y; c < nchunk; c += gridDim.y) lincomb_body(tk.a, blockIdx.x, c);
 }
 
 // Column-major copies between pitches, many in one launch (task blockIdx.y): used to give
