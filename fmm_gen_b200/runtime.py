@@ -164,6 +164,11 @@ class Plan:
     def from_levels(cls, algs, levels) -> "Plan":
         return cls(algebra.make_plan(algs, levels))
 
+    @property
+    def rank(self) -> int:
+        """Number of products R."""
+        return self.algebra.rank
+
     def bind_default(self) -> None:
         _check(self._lib.fmm_bind_default_plan(self.handle), "fmm_bind_default_plan")
 

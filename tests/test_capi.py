@@ -46,7 +46,7 @@ def test_library_exports_every_declared_symbol(lib):
 def test_plan_roundtrip_and_validation(lib):
     plan = algebra.make_plan(["222", "333"], [1, 1])
     p = runtime.Plan(plan)
-    assert lib.fmm_plan_rank(p.handle) == 161
+    assert lib.fmm_plan_rank(p.handle) == 161 == p.rank
     p.bind_default()
     assert lib.fmm_default_plan() == p.handle.value
     p.close()
