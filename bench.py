@@ -36,9 +36,11 @@ WORKLOAD = "222-1x333-1 abc FP64 C+=A*B over 16384^3, 14400x14400x480, 4000x1600
 METRIC = "effective TFLOPS (2mnk/t), 222-1x333-1 abc FP64"
 UNIT = "TFLOP/s"
 CPU_SAMPLE = (14400, 14400, 480)
-# DRAM traffic of one fmm_gemm_kernel launch per unit of work, from the ncu capture
-# summarised in profiles/ (bytes per executed core flop); None until captured.
-TRAFFIC_BYTES_PER_FLOP = None
+# DRAM traffic of the FMM products launches per executed core flop, from a one-pass ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of one timed step of this workload:
+# 257.1 GB over 6.88e12 executed flops (16384^3: 180.9 GB, 14400x14400x480: 58.0 GB,
+# 4000x16000x2000: 18.2 GB), summarised in profiles/.
+TRAFFIC_BYTES_PER_FLOP = 257.1e9 / 6.88e12
 
 
 def effective_flops(shapes):
