@@ -46,13 +46,14 @@ enum KernelKind {
   K_GEMM_BATCH = 6,
   K_LINCOMB_BATCH = 7,
   K_PITCH_COPY = 8,
-  K_NUM = 9
+  K_COMBINE = 9,
+  K_NUM = 10
 };
 const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
                                          "fmm_lincomb_kernel", "fmm_scatter_kernel",
                                          "fmm_split_operands_kernel", "fmm_split_gemm_kernel",
                                          "fmm_gemm_batch_kernel", "fmm_lincomb_batch_kernel",
-                                         "fmm_pitch_copy_kernel"};
+                                         "fmm_pitch_copy_kernel", "fmm_combine_kernel"};
 struct ProfRec {
   int kind;
   cudaEvent_t e0, e1;
@@ -107,6 +108,7 @@ struct fmm_plan {
   std::vector<int> ent_r;
   std::vector<double> ent_w;
   int n_cblk = 0;
+  int n_cterms = 0;  // C terms over all products
   // Pre-summed form: each product's A operand is either its single A block (src 0) or
   // slot j of the workspace S (src 1) that holds sum_i U[i,r] A_i; likewise for B / T.
   std::vector<fmm::Prod> prods_ps;
@@ -222,6 +224,7 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
     }
     p->prods.push_back(pr);
   }
+  for (const auto& pr : p->prods) p->n_cterms += pr.nc;
   // C block lists for the scatter (products in increasing order per block).
   const int nblk = dims[0] * dims[2];
   std::vector<std::vector<std::pair<int, double>>> lists(nblk);
@@ -491,6 +494,53 @@ int peel(int m, int n, int k, const double* A, long long lda, const double* B, l
   return FMM_OK;
 }
 
+// C_l += sum_r W[l,r] * M_r for every C block at once (fmm_combine_kernel); false when the
+// plan is too large for its shared-memory tables (the caller then uses the per-block scatter).
+bool combine_fits(const fmm_plan* plan) {
+  const int nblk = plan->dims[0] * plan->dims[2];
+  return nblk <= fmm::COMBINE_MAX_BLOCKS && plan->n_cterms <= fmm::COMBINE_MAX_TERMS &&
+         fmm::combine_smem_bytes(nblk, plan->n_cterms, plan->rank) <= 200 * 1024;
+}
+
+bool combine_configured[kMaxDevices];
+
+int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long long ldc, int ms, int ns,
+                   const double* M, long long ldm, long long m_stride, cudaStream_t st) {
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (!combine_configured[dev]) {
+      FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
+      combine_configured[dev] = true;
+    }
+  }
+  fmm::CombineArgs ca{};
+  ca.C = C;
+  ca.ldc = ldc;
+  ca.ms = ms;
+  ca.ns = ns;
+  ca.M = M;
+  ca.ldm = ldm;
+  ca.m_stride = m_stride;
+  ca.prods = d.prods;
+  ca.terms = d.terms;
+  ca.nprod = plan->rank;
+  ca.nterms = plan->n_cterms;
+  ca.grid_m = plan->dims[0];
+  ca.grid_n = plan->dims[2];
+  const size_t smem = fmm::combine_smem_bytes(ca.grid_m * ca.grid_n, ca.nterms, ca.nprod);
+  const long long blocks = ((long long)ms * ns + fmm::COMBINE_THREADS - 1) / fmm::COMBINE_THREADS;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 8));
+  {
+    ProfScope pf(K_COMBINE, st);
+    fmm::fmm_combine_kernel<<<grid, fmm::COMBINE_THREADS, smem, st>>>(ca);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cuda_status(cudaGetLastError());
+}
+
 // Pre-summing pays off once the sub-blocks are large enough that the extra pass over HBM
 // (each operand sum written once, then read by every tile that uses it) costs less than
 // folding the sums while staging, which limits the producer warps.  Measured on B200:
@@ -664,7 +714,9 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
           }
         }
       }
-      if (rc == FMM_OK) {
+      if (rc == FMM_OK && combine_fits(plan)) {
+        rc = launch_combine(plan, *d, C, ldc, ms, ns, M, ms, mstride, st);
+      } else if (rc == FMM_OK) {
         fmm::ScatterArgs sa{};
         sa.C = C;
         sa.ldc = ldc;
@@ -1196,9 +1248,13 @@ bool make_plane_map(CUtensorMap* map, const __nv_bfloat16* base, long long rows,
 
 // One split-BF16 launch pair over sub-blocks ms x ks x ns of a plan (R products):
 // operand planes into a stream-ordered workspace, then the persistent tcgen05 GEMM.
-int split_core(const DevTables& d, int R, const float* A, long long lda, const float* B, long long ldb, double* C,
-               long long ldc, int ms, int ns, int ks, cudaStream_t st) {
+int split_core(const fmm_plan* plan, const DevTables& d, const float* A, long long lda, const float* B,
+               long long ldb, double* C, long long ldc, int ms, int ns, int ks, cudaStream_t st) {
   if (ms <= 0 || ns <= 0 || ks <= 0) return FMM_OK;
+  const int R = plan->rank;
+  // several products: store each M_r, then one combine pass applies W (no C loads in the
+  // tensor-core kernel's epilogue); a single product goes straight into C
+  const bool use_m = R > 1 && combine_fits(plan);
   int dev = 0;
   int rc = split_configure(&dev);
   if (rc != FMM_OK) return rc;
@@ -1212,12 +1268,14 @@ int split_core(const DevTables& d, int R, const float* A, long long lda, const f
     return FMM_E_UNSUPPORTED;
   const size_t bytes_a = sizeof(__nv_bfloat16) * (size_t)(rows_a * kpad);
   const size_t bytes_b = sizeof(__nv_bfloat16) * (size_t)(rows_b * kpad);
-  const size_t bytes_t = R > 1 ? sizeof(int) * (size_t)ntiles : 0;
+  const size_t bytes_m = use_m ? sizeof(double) * (size_t)R * ms * ns : 0;
+  const size_t bytes_t = (R > 1 && !use_m) ? sizeof(int) * (size_t)ntiles : 0;
   char* ws = nullptr;
-  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes_a + bytes_b + bytes_t + 16, st));
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes_a + bytes_b + bytes_m + bytes_t + 16, st));
   __nv_bfloat16* PA = reinterpret_cast<__nv_bfloat16*>(ws);
   __nv_bfloat16* PB = reinterpret_cast<__nv_bfloat16*>(ws + bytes_a);
-  int* tickets = R > 1 ? reinterpret_cast<int*>(ws + bytes_a + bytes_b) : nullptr;
+  double* Mws = use_m ? reinterpret_cast<double*>(ws + bytes_a + bytes_b) : nullptr;
+  int* tickets = bytes_t ? reinterpret_cast<int*>(ws + bytes_a + bytes_b + bytes_m) : nullptr;
   if (tickets) rc = cuda_status(cudaMemsetAsync(tickets, 0, bytes_t, st));
 
   fmms::SplitArgs sa{};
@@ -1266,6 +1324,9 @@ int split_core(const DevTables& d, int R, const float* A, long long lda, const f
     g.tiles_m = tiles_m;
     g.tiles_n = tiles_n;
     g.tickets = tickets;
+    g.M = Mws;
+    g.ldm = ms;
+    g.m_stride = (long long)ms * ns;
     g.status = dev_status[dev];
     const long long units = ntiles * R;
     const unsigned grid = (unsigned)(units < sm_count[dev] ? units : sm_count[dev]);
@@ -1276,6 +1337,7 @@ int split_core(const DevTables& d, int R, const float* A, long long lda, const f
     g_launches.fetch_add(1, std::memory_order_relaxed);
     rc = cuda_status(cudaGetLastError());
   }
+  if (rc == FMM_OK && use_m) rc = launch_combine(plan, d, C, ldc, ms, ns, Mws, ms, (long long)ms * ns, st);
   cudaError_t fe = cudaFreeAsync(ws, st);
   if (rc == FMM_OK) rc = cuda_status(fe);
   return rc;
@@ -1287,7 +1349,7 @@ int split_plain(int m, int n, int k, const float* A, long long lda, const float*
   DevTables* d = nullptr;
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
-  return split_core(*d, 1, A, lda, B, ldb, C, ldc, m, n, k, st);
+  return split_core(classical_plan(), *d, A, lda, B, ldb, C, ldc, m, n, k, st);
 }
 
 int run_split(const fmm_plan* plan, int m, int n, int k, const float* A, long long lda, const float* B,
@@ -1302,8 +1364,8 @@ int run_split(const fmm_plan* plan, int m, int n, int k, const float* A, long lo
     DevTables* d = nullptr;
     rc = device_tables(plan, &d);
     if (rc != FMM_OK) return rc;
-    rc = split_core(*d, plan->rank, A, lda, B, ldb, C, ldc, md / plan->dims[0], nd / plan->dims[2],
-                    kd / plan->dims[1], st);
+    rc = split_core(plan, *d, A, lda, B, ldb, C, ldc, md / plan->dims[0], nd / plan->dims[2], kd / plan->dims[1],
+                    st);
     if (rc != FMM_OK) return rc;
   }
   // fringe strips: the same regions, in the same order, as the FP64 path's peeling

@@ -1049,6 +1049,103 @@ __global__ void fmm_lincomb_batch_kernel(const LincombTask* tasks) {
   for (long long c = blockIdx.y; c < nchunk; c += gridDim.y) lincomb_body(tk.a, blockIdx.x, c);
 }
 
+// C_l += sum_r W[l, r] * M_r for every C block l of the plan's grid at once: a thread owns
+// one element position, keeps the running value of that position in every C block in
+// shared memory (loaded from C first), and applies the products in order r = 0..R-1 with
+// the same fma sequence as the epilogue's multi-destination update.  Each M_r and each C
+// element cross HBM once: bytes per position 8 (R + 2 * blocks).  The product -> (block,
+// coefficient) table is staged in shared memory once per CTA.
+struct CombineArgs {
+  double* C;
+  long long ldc;
+  int ms, ns;
+  const double* M;
+  long long ldm;
+  long long m_stride;
+  const Prod* prods;
+  const Term* terms;
+  int nprod;
+  int nterms;          // C terms over all products (sum of nc)
+  int grid_m, grid_n;  // C block grid
+};
+
+constexpr int COMBINE_THREADS = 256;
+constexpr int COMBINE_MAX_BLOCKS = 64;
+constexpr int COMBINE_MAX_TERMS = 4096;
+constexpr int COMBINE_BATCH = 8;
+
+__host__ __device__ constexpr size_t combine_smem_bytes(int nblk, int nterms, int nprod) {
+  return sizeof(double) * (size_t)nblk * COMBINE_THREADS + (sizeof(double) + sizeof(int)) * (size_t)nterms +
+         sizeof(int) * (size_t)(nprod + 1);
+}
+
+__global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const CombineArgs a) {
+  extern __shared__ __align__(16) double cacc[];
+  const int nblk = a.grid_m * a.grid_n;
+  double* tcoef = cacc + (size_t)nblk * COMBINE_THREADS;
+  int* tblk = reinterpret_cast<int*>(tcoef + a.nterms);
+  int* tfirst = tblk + a.nterms;  // compact C-term ranges per product, nprod + 1 entries
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < a.nprod; ++r) {
+      tfirst[r] = acc;
+      acc += a.prods[r].nc;
+    }
+    tfirst[a.nprod] = acc;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < a.nprod; r += blockDim.x) {
+    const Prod p = a.prods[r];
+    for (int c = 0; c < p.nc; ++c) {
+      const Term t = a.terms[p.c0 + c];
+      tcoef[tfirst[r] + c] = t.coef;
+      tblk[tfirst[r] + c] = t.row * a.grid_n + t.col;
+    }
+  }
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const long long total = (long long)a.ms * a.ns;
+  for (long long e0 = (long long)blockIdx.x * COMBINE_THREADS; e0 < total; e0 += (long long)gridDim.x * COMBINE_THREADS) {
+    const long long e = e0 + tid;
+    if (e >= total) continue;
+    const int i = (int)(e % a.ms);
+    const long long j = e / a.ms;
+    // loads in groups of COMBINE_BATCH independent ones, so each thread keeps that many in
+    // flight (a bandwidth-bound pass needs the memory parallelism)
+    for (int b0 = 0; b0 < nblk; b0 += COMBINE_BATCH) {
+      double v[COMBINE_BATCH];
+#pragma unroll
+      for (int q = 0; q < COMBINE_BATCH; ++q) {
+        const int b = b0 + q;
+        v[q] = b < nblk ? a.C[(long long)(b / a.grid_n) * a.ms + i + ((long long)(b % a.grid_n) * a.ns + j) * a.ldc]
+                        : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < COMBINE_BATCH; ++q)
+        if (b0 + q < nblk) cacc[(size_t)(b0 + q) * COMBINE_THREADS + tid] = v[q];
+    }
+    for (int r0 = 0; r0 < a.nprod; r0 += COMBINE_BATCH) {
+      double m[COMBINE_BATCH];
+#pragma unroll
+      for (int q = 0; q < COMBINE_BATCH; ++q)
+        m[q] = r0 + q < a.nprod ? a.M[(long long)(r0 + q) * a.m_stride + i + j * a.ldm] : 0.0;
+#pragma unroll
+      for (int q = 0; q < COMBINE_BATCH; ++q) {
+        const int r = r0 + q;
+        if (r >= a.nprod) break;
+        for (int c = tfirst[r]; c < tfirst[r + 1]; ++c) {
+          double* x = cacc + (size_t)tblk[c] * COMBINE_THREADS + tid;
+          *x = fma(tcoef[c], m[q], *x);
+        }
+      }
+    }
+    for (int b = 0; b < nblk; ++b) {
+      const int br = b / a.grid_n, bc = b % a.grid_n;
+      a.C[(long long)br * a.ms + i + ((long long)bc * a.ns + j) * a.ldc] = cacc[(size_t)b * COMBINE_THREADS + tid];
+    }
+  }
+}
+
 // Column-major copies between pitches, many in one launch (task blockIdx.y): used to give
 // operands with an odd leading dimension the even pitch (16-byte column starts) that
 // tensor-memory-access staging needs.

@@ -13,8 +13,9 @@
 //      into one, the five smaller products into another, so that the accumulators' own
 //      rounding never drops the small terms against the large ones.  Every 128-deep k
 //      chunk is drained with tcgen05.ld (the two accumulators added once in FP32) and
-//      added into FP64 registers, so FP32 rounding only acts within a chunk; the epilogue
-//      adds W[l,r] * M_r into FP64 C.
+//      added into FP64 registers, so FP32 rounding only acts within a chunk.  With several
+//      products the epilogue stores M_r (FP64) to a workspace and fmm_combine_kernel adds
+//      W[l,r] * M_r into C afterwards; a single product is added into C directly.
 //
 // Work unit = (128 x 128 tile position, product r); a unit owns its tile position in every
 // C block, and per-tile tickets order the products' C updates (no atomics on C, the result
@@ -76,6 +77,9 @@ struct SplitGemmArgs {
   int nprod;
   int tiles_m, tiles_n;
   int* tickets;      // per tile: products whose C updates are done (zeroed before launch)
+  double* M;         // when set: product r's tile is stored to M + r * m_stride (ld ldm) instead
+  long long ldm;     // of being added into C; a combine pass applies W afterwards
+  long long m_stride;
   unsigned* status;
 };
 
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
     const int et = tid - 128;
     const int quarter = warp & 3, half = (warp - 4) >> 2;
     const int row = quarter * 32 + lane;
-    const bool ordered = a.nprod > 1;
+    const bool ordered = a.nprod > 1 && a.M == nullptr;
     long long ch = 0;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
       const SUnit w = s_decode(a, u);
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
       const Prod p = a.prods[w.r];
       const int nch = (nks + DRAIN_STAGES - 1) / DRAIN_STAGES;
       for (int c = 0; c < nch; ++c, ++ch) {
-        if (c == (nch > C_PREFETCH_CHUNKS ? nch - C_PREFETCH_CHUNKS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, et);
+        if (!a.M && c == (nch > C_PREFETCH_CHUNKS ? nch - C_PREFETCH_CHUNKS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, et);
         const int b = (int)(ch % NACC);
         fmm::mbar_wait(accf0 + 8 * b, (unsigned)((ch / NACC) & 1), a.status);
         tc_fence_after();
@@ -311,6 +315,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
         tc_fence_before();
         __syncwarp();
         if (lane == 0) fmm::mbar_arrive(acce0 + 8 * b);
+      }
+      if (a.M) {  // store-only epilogue: no loads, so it does not hold up the next drains
+        const int rr = w.m0 + row;
+        if (rr < a.ms) {
+          double* Mr = a.M + (long long)w.r * a.m_stride + rr;
+#pragma unroll
+          for (int j = 0; j < 64; ++j) {
+            const int cc = w.n0 + half * 64 + j;
+            if (cc < a.ns) Mr[(long long)cc * a.ldm] = acc[j];
+          }
+        }
+        continue;
       }
       // this tile position's updates from products < r are complete
       if (ordered && w.r > 0) {

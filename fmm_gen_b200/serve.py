@@ -74,7 +74,8 @@ def request_bytes(kind: str, shape: Sequence[int], algorithm: str) -> int:
         dims = plan.dims if plan is not None else (1, 1, 1)
         ms, ks, ns = m // dims[0], k // dims[1], n // dims[2]
         kpad = -(-ks // 64) * 64
-        return 4 * (m * k + k * n) + 8 * m * n + 6 * R * (ms + ns) * kpad
+        mws = 8 * R * ms * ns if R > 1 else 0  # product tiles before the combine pass
+        return 4 * (m * k + k * n) + 8 * m * n + 6 * R * (ms + ns) * kpad + mws
     ws = 0
     plan = tuner.plan_of(algorithm)
     if plan is not None:

@@ -128,8 +128,9 @@ int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const doubl
  * accumulated in FP32 over 128-deep k chunks and in FP64 across chunks; W[l,r] * M_r is
  * added to C in FP64.  Relative Frobenius error against the FP64 product of the same
  * FP32 inputs: about 1e-7 (classical) and a few 1e-7 for two Strassen levels.
- * Workspace: 6 R (ms + ns) kpad bytes from the stream-ordered allocator
- * (kpad = ks rounded up to 64). */
+ * Workspace from the stream-ordered allocator: 6 R (ms + ns) kpad bytes of bf16 planes
+ * (kpad = ks rounded up to 64) and, for R > 1, 8 R ms ns bytes of product tiles that a
+ * final pass adds into C. */
 int fmm_split_gemm_dev(const fmm_plan *plan, int m, int n, int k, const float *A, long lda, const float *B,
                        long ldb, double *C, long ldc, void *stream);
 
