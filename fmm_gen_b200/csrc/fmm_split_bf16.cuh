@@ -20,7 +20,7 @@
 // Work unit = (128 x 128 tile position, product r); a unit owns its tile position in every
 // C block, and per-tile tickets order the products' C updates (no atomics on C, the result
 // does not depend on scheduling).  Warp roles (384 threads, one CTA per SM, persistent):
-// warp 0 lane 0 issues TMA (128-byte swizzle, no multicast), warp 1 owns tensor memory and
+// warp 0 lane 0 issues TMA (128-byte swizzle, each CTA loads its own tiles), warp 1 owns tensor memory and
 // its lane 0 issues the MMAs, warps 4..11 drain the accumulator and run the epilogue.
 // Every wait is bounded; tensor memory is freed on every path.
 #pragma once

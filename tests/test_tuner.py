@@ -5,6 +5,8 @@ The model's per-algorithm counts follow the reference's model (model_coefficient
 project's own.  The search is exercised with a synthetic measure function."""
 import math
 
+import pytest
+
 from fmm_gen_b200 import tuner
 
 
@@ -61,3 +63,15 @@ def test_search_without_measurement_returns_the_model_choice():
     shapes = tuner.random_batch_shapes(16, seed=1)
     rep = tuner.BatchTuner().tune(shapes)
     assert rep.choices == rep.model_choices
+
+
+def test_sweep_families_match_the_reference_ranges():
+    from fmm_gen_b200 import sweep
+
+    assert sweep.shapes("square", [240, 480]) == [(240, 240, 240), (480, 480, 480)]
+    assert sweep.shapes("rankk", [240]) == [(14400, 14400, 240)]
+    assert sweep.shapes("fixk", [960]) == [(960, 960, 1024)]
+    with pytest.raises(ValueError):
+        sweep.shapes("cube", [1])
+    m = tuner.B200Model()
+    assert sweep.model_gflops("222-1", 8192, 8192, 8192, m) > sweep.model_gflops("classical", 8192, 8192, 8192, m)
