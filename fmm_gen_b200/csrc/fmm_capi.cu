@@ -307,6 +307,8 @@ int configure_kernel(int* dev_out) {
                                       (int)fmm::smem_bytes(false)));
     FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fmm::smem_bytes(true)));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fmm::SMEM_BYTES_DIRECT));
     if (!g_encode_tiled) {
       cudaDriverEntryPointQueryResult q;
       void* fn = nullptr;
@@ -369,10 +371,13 @@ struct PresumOps {
   int nslotB = 0;
 };
 
+// direct_ok: every product's operands are single unit-coefficient blocks (pre-summed
+// products, the classical plan), so with TMA staging and whole k steps the direct variant
+// (epilogue on the otherwise idle folding warps, overlapping the next product) can run.
 int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
                 int mode, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
                 double* C, long long ldc, double* M, long long ldm, long long m_stride, int ms, int ns, int ks,
-                cudaStream_t st) {
+                cudaStream_t st, bool direct_ok = false) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
   int dev = 0;
   int rc = configure_kernel(&dev);
@@ -431,9 +436,12 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
   }
+  const bool direct = direct_ok && tma && mode == fmm::MODE_ACCUM_C && ks % fmm::BK == 0;
   {
     ProfScope ps(kind, st);
-    if (tma)
+    if (direct)
+      fmm::fmm_gemm_direct_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES_DIRECT, st>>>(a);
+    else if (tma)
       fmm::fmm_gemm_kernel<true><<<grid, fmm::NTHREADS, fmm::smem_bytes(true), st>>>(a);
     else
       fmm::fmm_gemm_kernel<false><<<grid, fmm::NTHREADS, fmm::smem_bytes(false), st>>>(a);
@@ -456,7 +464,7 @@ int plain_gemm(int m, int n, int k, const double* A, long long lda, const double
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
   return launch_gemm(K_GEMM_CLASSICAL, d->prods, d->terms, kUnitGrid, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb,
-                     PresumOps{}, C, ldc, nullptr, 0, 0, m, n, k, st);
+                     PresumOps{}, C, ldc, nullptr, 0, 0, m, n, k, st, true);
 }
 
 int grid_for(long long total, int threads) {
@@ -640,7 +648,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         rc = presum(*d, A, lda, B, ldb, ps, ms, ns, ks, st);
         if (rc == FMM_OK)
           rc = launch_gemm(K_GEMM_FMM, d->prods_ps, d->terms_ps, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
-                           ps, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
+                           ps, C, ldc, nullptr, 0, 0, ms, ns, ks, st, true);
         cudaError_t fe = cudaFreeAsync(ws, st);
         if (rc == FMM_OK) rc = cuda_status(fe);
       } else {

@@ -961,6 +961,232 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_batch_kernel(const Batch
   gemm_cta<TMA>(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status});
 }
 
+// ------------------------------------------------------------------------------------
+// Direct variant: every operand of every product is one unit-coefficient block staged by
+// TMA straight into the stage (the pre-summed ABC path and the classical plan) and ks is a
+// multiple of BK, so no term is folded.  The seven folding warps then run the
+// multi-destination C epilogue instead: the consumers write each finished product tile
+// into shared memory (one 128 x 128 FP64 buffer, in place of the raw slots and two of the
+// stages) and go straight on with the next product, while warps 1..7 add W[l,r] * M_r into
+// the C blocks from it.  The epilogue overlaps the DMMAs of the next product.
+// ------------------------------------------------------------------------------------
+constexpr int NSTAGE_D = 4;
+constexpr int MS_LD = BM + 1;  // product tile in shared memory: column-major, padded
+constexpr int NEPI_D = NFOLD;  // epilogue threads (warps 1..7)
+static_assert((size_t)(NSTAGE_D * STAGE_SZ + BN * (BM + 1)) * sizeof(double) + 80 <= 232448, "direct variant shared memory");
+constexpr size_t SMEM_BYTES_DIRECT =
+    (size_t)(NSTAGE_D * STAGE_SZ + BN * MS_LD) * sizeof(double) + (2 * NSTAGE_D + 2) * sizeof(unsigned long long);
+
+template <class Src>
+__device__ __forceinline__ void direct_issuer(const Src& src, double* stages, unsigned full0, unsigned empty0) {
+  LoadIter it;
+  load_iter_start(src, it);
+  long long kc = 0;
+  int mapped = -1;
+#pragma unroll 1
+  while (it.valid) {
+    const GemmArgs& a = src.get(it.j);
+    if (it.j != mapped) {
+      src.acquire_maps(it.j);
+      mapped = it.j;
+    }
+    const int stage = (int)(kc % NSTAGE_D);
+    double* opA = stages + (size_t)stage * STAGE_SZ;
+    const int k0 = it.s * BK;
+    mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE_D) & 1) ^ 1), src.status());
+    const unsigned fb = full0 + 8 * stage;
+    mbar_arrive_expect_tx(fb, TMA_BYTES_A + TMA_BYTES_B8);
+    tma_load_2d(smem_u32(opA), it.ta.src ? &a.tmAw : &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, fb);
+    tma_load_2d(smem_u32(opA + OPA_SZ), it.tb.src ? &a.tmBw : &a.tmB, it.tb.row * a.ks + k0,
+                it.tb.col * a.ns + it.w.n0, fb);
+    ++kc;
+    kiter_next(src, it);
+  }
+}
+
+template <class Src>
+__device__ __forceinline__ void direct_consumer(const Src& src, const double* stages, double* Ms, unsigned full0,
+                                                unsigned empty0, unsigned mfull, unsigned mempty, int ct) {
+  const int warp = ct >> 5, lane = ct & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int nunits = src.total();
+  long long kc = 0, q = 0;
+  double acc[4][4][4];
+#pragma unroll 1
+  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const int job = src.find(u);
+    const GemmArgs& a = src.get(job);
+    const int nks = (a.ks + BK - 1) / BK;
+    const Unit w = decode_unit(a, u - src.first_unit(job));
+#pragma unroll 1
+    for (int r = w.r0; r < w.r1; ++r, ++q) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+#pragma unroll 1
+      for (int s = 0; s < nks; ++s, ++kc) {
+        const int stage = (int)(kc % NSTAGE_D);
+        const double* opA = stages + (size_t)stage * STAGE_SZ;
+        mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
+        mma_stage(opA, opA + OPA_SZ, acc, wm, wn, g, t4);
+        __threadfence_block();  // fragment loads complete before the stage can be refilled
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * stage);
+      }
+      // hand the product tile to the epilogue warps once they are done with the previous one
+      mbar_wait(mempty, (unsigned)((q & 1) ^ 1), src.status());
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int rr = wm * 64 + i * 16 + g + 8 * h;
+              const int cc = wn * 32 + j * 8 + t4 * 2 + e;
+              Ms[cc * MS_LD + rr] = acc[i][j][2 * h + e];
+            }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(mfull);
+    }
+  }
+}
+
+template <class Src>
+__device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms, unsigned mfull, unsigned mempty,
+                                                int et) {
+  const int ew = et >> 5, lane = et & 31;
+  constexpr int NW = NEPI_D / 32;  // 7 warps
+  const int nunits = src.total();
+  long long q = 0;
+#pragma unroll 1
+  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const int job = src.find(u);
+    const GemmArgs& a = src.get(job);
+    const int ul = u - src.first_unit(job);
+    const int ntiles = a.tiles_m * a.tiles_n;
+    const bool ordered = (a.mode == MODE_ACCUM_C) && a.chunks > 1;
+    const Unit w = decode_unit(a, ul);
+    const int chunk = ul / ntiles;
+#pragma unroll 1
+    for (int r = w.r0; r < w.r1; ++r, ++q) {
+      const Prod p = a.prods[r];
+      // the unit's C tiles into L2 while its product is still being computed
+      for (int c = 0; c < p.nc; ++c) {
+        const Term tm = a.terms[p.c0 + c];
+        const double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc;
+        for (int l = et; l < (BM / 16) * BN; l += NEPI_D) {
+          const int rr = w.m0 + (l % (BM / 16)) * 16, cc = w.n0 + l / (BM / 16);
+          if (rr < a.ms && cc < a.ns) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Cb + rr + (long long)cc * a.ldc));
+        }
+      }
+      mbar_wait(mfull, (unsigned)(q & 1), src.status());
+      if (ordered && r == w.r0) {
+        if (et == 0) {
+          const int* tp = a.tickets + w.tile;
+          if (ld_acquire(tp) < chunk) {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(tp) < chunk) {
+              if (*(volatile unsigned*)a.status != 0u) break;
+              if (global_ns() - t0 > WAIT_LIMIT_NS) {
+                atomicOr(a.status, STATUS_TICKET_TIMEOUT);
+                break;
+              }
+              __nanosleep(256);
+            }
+          }
+        }
+        named_bar_sync(2, NEPI_D);
+      }
+      // C_l += w * M_r: warp ew takes columns ew, ew + 7, ... four at a time; a lane owns rows
+      // lane, lane + 32, lane + 64, lane + 96, so loads and stores are 256-byte coalesced and
+      // 16 loads are in flight per lane before the stores
+#pragma unroll 1
+      for (int c = 0; c < p.nc; ++c) {
+        const Term tm = a.terms[p.c0 + c];
+        const double wgt = tm.coef;
+        double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc + w.m0 + lane;
+        const int rmax = a.ms - w.m0 - lane;  // rows of this lane inside the block: rr < rmax
+#pragma unroll 1
+        for (int col0 = ew; col0 < BN; col0 += NW * 4) {
+          double cv[4][4];
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            const int col = col0 + cb * NW;
+            const bool cok = col < BN && w.n0 + col < a.ns;
+            const double* cp = Cb + (long long)(w.n0 + col) * a.ldc;
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) cv[cb][ch] = (cok && ch * 32 < rmax) ? cp[ch * 32] : 0.0;
+          }
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            const int col = col0 + cb * NW;
+            if (!(col < BN && w.n0 + col < a.ns)) continue;
+            double* cp = Cb + (long long)(w.n0 + col) * a.ldc;
+            const double* mp = Ms + col * MS_LD + lane;
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch)
+              if (ch * 32 < rmax) cp[ch * 32] = fma(wgt, mp[ch * 32], cv[cb][ch]);
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(mempty);  // the buffer can take the next product
+    }
+    if (ordered) {
+      __threadfence();
+      named_bar_sync(2, NEPI_D);
+      if (et == 0) st_release(a.tickets + w.tile, chunk + 1);
+    }
+  }
+}
+
+template <class Src>
+__device__ __forceinline__ void gemm_cta_direct(const Src& src) {
+  extern __shared__ __align__(128) double smem[];
+  double* stages = smem;                                        // [NSTAGE_D][STAGE_SZ]
+  double* Ms = stages + (size_t)NSTAGE_D * STAGE_SZ;            // [BN][MS_LD]
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(Ms + (size_t)BN * MS_LD);
+  const unsigned full0 = smem_u32(bars);
+  const unsigned empty0 = smem_u32(bars + NSTAGE_D);
+  const unsigned mfull = smem_u32(bars + 2 * NSTAGE_D);
+  const unsigned mempty = smem_u32(bars + 2 * NSTAGE_D + 1);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE_D; ++s) {
+      mbar_init(full0 + 8 * s, 1);             // the issuer's arrival + TMA bytes
+      mbar_init(empty0 + 8 * s, NCONS / 32);
+    }
+    mbar_init(mfull, NCONS / 32);
+    mbar_init(mempty, NEPI_D / 32);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid < NPROD) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
+    if (tid == 0)
+      direct_issuer(src, stages, full0, empty0);
+    else if (tid >= 32)
+      direct_epilogue(src, Ms, mfull, mempty, tid - 32);
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
+    direct_consumer(src, stages, Ms, full0, empty0, mfull, mempty, tid - NPROD);
+  }
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_direct_kernel(const __grid_constant__ GemmArgs a) {
+  gemm_cta_direct(OneJob{a});
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_direct_batch_kernel(const BatchArgs b) {
+  gemm_cta_direct(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status});
+}
+
 // Operand sums in HBM: out_j = sum_t coef_t * X_{blk_t} for the A terms (side 0) or the
 // B terms (side 1) of product plist[j] (j = blockIdx.y).  Used for the NAIVE pack
 // type's S_r / T_r temporaries and for the pre-summed operands of the ABC pack type.
