@@ -371,6 +371,13 @@ struct PresumOps {
   int nslotB = 0;
 };
 
+// Every k step of a product reads only its own operand blocks: ks is a multiple of BK, or
+// the block grid is 1 x 1 x 1, where the tensor maps end at the operands' last k column / row
+// and a partial last step reads TMA's zero fill.
+bool whole_k_steps(const int grid_dims[3], int ks) {
+  return ks % fmm::BK == 0 || (grid_dims[0] == 1 && grid_dims[1] == 1 && grid_dims[2] == 1);
+}
+
 // direct_ok: every product's operands are single unit-coefficient blocks (pre-summed
 // products, the classical plan), so with TMA staging and whole k steps the direct variant
 // (epilogue on the otherwise idle folding warps, overlapping the next product) can run.
@@ -436,7 +443,7 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
   }
-  const bool direct = direct_ok && tma && mode == fmm::MODE_ACCUM_C && ks % fmm::BK == 0;
+  const bool direct = direct_ok && tma && mode == fmm::MODE_ACCUM_C && whole_k_steps(grid_dims, ks);
   {
     ProfScope ps(kind, st);
     if (direct)
@@ -1421,6 +1428,7 @@ struct fmm_batch {
   std::vector<int> m, n, k;
   std::vector<const fmm_plan*> plans;
   std::vector<Job> jobs[2];        // phase 0: FMM cores and disjoint strips; phase 1: k strips
+  bool direct[2] = {true, true};   // every job of the phase can run the direct variant
   std::vector<int> unit_start[2];
   int max_slots = 0;
   unsigned max_lincomb_chunks = 1;
@@ -1457,6 +1465,8 @@ int batch_configure(int* dev) {
                                       (int)fmm::smem_bytes(true)));
     FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fmm::smem_bytes(false)));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_gemm_direct_batch_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fmm::SMEM_BYTES_DIRECT));
     batch_configured[*dev] = true;
   }
   return FMM_OK;
@@ -1508,6 +1518,9 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
   j.ticket_off = b->n_tickets;
   if (j.chunks > 1) b->n_tickets += (size_t)j.tiles_m * j.tiles_n;
   j.cost = (double)plan->rank / j.chunks * ((ks + fmm::BK - 1) / fmm::BK);
+  // direct staging: operands are single unit-coefficient blocks (pre-summed or classical)
+  // and every k step stays inside them
+  if (!((j.presum || plan->rank == 1) && whole_k_steps(j.grid, ks))) b->direct[phase] = false;
   b->jobs[phase].push_back(j);
 }
 
@@ -1812,7 +1825,9 @@ int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool t
     const unsigned grid = (unsigned)std::min<long long>(ba.units, sm_count[b->dev]);
     {
       ProfScope pf(K_GEMM_BATCH, st);
-      if (tma[ph])
+      if (tma[ph] && b->direct[ph])
+        fmm::fmm_gemm_direct_batch_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES_DIRECT, st>>>(ba);
+      else if (tma[ph])
         fmm::fmm_gemm_batch_kernel<true><<<grid, fmm::NTHREADS, fmm::smem_bytes(true), st>>>(ba);
       else
         fmm::fmm_gemm_batch_kernel<false><<<grid, fmm::NTHREADS, fmm::smem_bytes(false), st>>>(ba);
