@@ -93,6 +93,9 @@ struct DevTables {
   fmm::Term* terms_ps = nullptr;
   int* plistA = nullptr;          // products whose A operand is pre-summed, in slot order
   int* plistB = nullptr;
+  fmm::Prod* prods_all = nullptr;  // every product over pre-summed slots (slot r = product r)
+  fmm::Term* terms_all = nullptr;
+  int* plist_all = nullptr;        // 0 .. R-1
   bool ready = false;
 };
 
@@ -114,6 +117,10 @@ struct fmm_plan {
   std::vector<fmm::Prod> prods_ps;
   std::vector<fmm::Term> terms_ps;
   std::vector<int> plistA, plistB;
+  // Every product pre-summed (slot r = product r): used when ks is not a multiple of the
+  // k step, so that zero-padded workspaces keep each k step inside its operand block.
+  std::vector<fmm::Prod> prods_all;
+  std::vector<fmm::Term> terms_all;
   std::mutex mu;
   DevTables dev[kMaxDevices];
 };
@@ -163,6 +170,16 @@ int upload_tables(fmm_plan* p, DevTables& d) {
     FMM_CUDA_TRY(cudaMemcpy(d.plistA, p->plistA.data(), sizeof(int) * p->plistA.size(), cudaMemcpyHostToDevice));
   if (!p->plistB.empty())
     FMM_CUDA_TRY(cudaMemcpy(d.plistB, p->plistB.data(), sizeof(int) * p->plistB.size(), cudaMemcpyHostToDevice));
+  std::vector<int> all(p->rank);
+  for (int r = 0; r < p->rank; ++r) all[r] = r;
+  FMM_CUDA_TRY(cudaMalloc(&d.prods_all, sizeof(fmm::Prod) * p->prods_all.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.terms_all, sizeof(fmm::Term) * p->terms_all.size()));
+  FMM_CUDA_TRY(cudaMalloc(&d.plist_all, sizeof(int) * all.size()));
+  FMM_CUDA_TRY(cudaMemcpy(d.prods_all, p->prods_all.data(), sizeof(fmm::Prod) * p->prods_all.size(),
+                          cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemcpy(d.terms_all, p->terms_all.data(), sizeof(fmm::Term) * p->terms_all.size(),
+                          cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemcpy(d.plist_all, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
   d.ready = true;
   return FMM_OK;
 }
@@ -272,6 +289,17 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
     q.nc = pr.nc;
     for (int c = 0; c < pr.nc; ++c) p->terms_ps.push_back(p->terms[pr.c0 + c]);
     p->prods_ps.push_back(q);
+    fmm::Prod qa{};
+    qa.a0 = (int)p->terms_all.size();
+    qa.na = 1;
+    p->terms_all.push_back(fmm::Term{0, r, 1.0, 1, 0});
+    qa.b0 = (int)p->terms_all.size();
+    qa.nb = 1;
+    p->terms_all.push_back(fmm::Term{0, r, 1.0, 1, 0});
+    qa.c0 = (int)p->terms_all.size();
+    qa.nc = pr.nc;
+    for (int c = 0; c < pr.nc; ++c) p->terms_all.push_back(p->terms[pr.c0 + c]);
+    p->prods_all.push_back(qa);
   }
   *out = p;
   return FMM_OK;
@@ -363,6 +391,9 @@ int choose_chunks(int ntiles, int nprod, int nsm) {
 // Launch the persistent DMMA GEMM over sub-blocks of size ms x ks x ns.
 // Workspaces of pre-summed operands (slot j of S: ms x ks, of T: ks x ns, block columns).
 struct PresumOps {
+  const int* plistA = nullptr;  // products of the slots (device); nullptr: the plan's lists
+  const int* plistB = nullptr;
+  int kslot = 0;                // columns per S slot and rows per T slot; 0: ks
   const double* S = nullptr;
   long long ldS = 0;
   int nslotA = 0;
@@ -384,7 +415,7 @@ bool whole_k_steps(const int grid_dims[3], int ks) {
 int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
                 int mode, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
                 double* C, long long ldc, double* M, long long ldm, long long m_stride, int ms, int ns, int ks,
-                cudaStream_t st, bool direct_ok = false) {
+                cudaStream_t st, bool direct_ok = false, int ks_orig = -1) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
   int dev = 0;
   int rc = configure_kernel(&dev);
@@ -425,7 +456,9 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
   a.tickets = tickets;
   const unsigned grid = (unsigned)(units < sm_count[dev] ? units : sm_count[dev]);
   // A spans grid_dims[0] x grid_dims[1] blocks of ms x ks; B grid_dims[1] x grid_dims[2] of ks x ns
-  const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * ks,
+  // the operands' own maps cover the operands (their k extent is the real one when the
+  // products read zero-padded pre-summed slots)
+  const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * (ks_orig >= 0 ? ks_orig : ks),
                   bn = (long long)grid_dims[2] * ns;
   bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
              make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
@@ -578,10 +611,10 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     la.blk_col_stride = ks;
     la.out = const_cast<double*>(ps.S);
     la.ldo = ps.ldS;
-    la.out_stride = ps.ldS * ks;
+    la.out_stride = ps.ldS * (ps.kslot ? ps.kslot : ks);
     la.prods = d.prods;
     la.terms = d.terms;
-    la.plist = d.plistA;
+    la.plist = ps.plistA ? ps.plistA : d.plistA;
     la.side = 0;
     const dim3 g((unsigned)ps.nslotA, lincomb_chunks((long long)(ms + 1) / 2 * ks));
     ProfScope pf(K_LINCOMB, st);
@@ -601,7 +634,7 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     lb.out_stride = ps.ldT * ns;
     lb.prods = d.prods;
     lb.terms = d.terms;
-    lb.plist = d.plistB;
+    lb.plist = ps.plistB ? ps.plistB : d.plistB;
     lb.side = 1;
     const dim3 g((unsigned)ps.nslotB, lincomb_chunks((long long)(ks + 1) / 2 * ns));
     ProfScope pf(K_LINCOMB, st);
@@ -637,7 +670,37 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
       const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
-      if (use_presum(plan, ms, ns, ks)) {
+      if (use_presum(plan, ms, ns, ks) && ks % fmm::BK != 0) {
+        // Every product pre-summed into slots whose k extent is padded with zeros to a
+        // multiple of the k step: all k steps are whole, so the direct variant runs.
+        const int kp = (ks + fmm::BK - 1) / fmm::BK * fmm::BK;
+        PresumOps ps;
+        ps.plistA = d->plist_all;
+        ps.plistB = d->plist_all;
+        ps.kslot = kp;
+        const size_t sbytes = sizeof(double) * (size_t)ms * kp * R;
+        const size_t tbytes = sizeof(double) * (size_t)kp * ns * R;
+        char* ws = nullptr;
+        FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, sbytes + tbytes + 16, st));
+        ps.S = reinterpret_cast<double*>(ws);
+        ps.ldS = ms;
+        ps.nslotA = R;
+        ps.T = reinterpret_cast<double*>(ws + sbytes);
+        ps.ldT = kp;
+        ps.nslotB = R;
+        // zero padding: S slot r columns [ks, kp); T rows [ks, kp) of every column
+        rc = cuda_status(cudaMemset2DAsync(ws + sizeof(double) * (size_t)ms * ks, sizeof(double) * (size_t)ms * kp, 0,
+                                           sizeof(double) * (size_t)ms * (kp - ks), R, st));
+        if (rc == FMM_OK)
+          rc = cuda_status(cudaMemset2DAsync(ws + sbytes + sizeof(double) * ks, sizeof(double) * kp, 0,
+                                             sizeof(double) * (kp - ks), (size_t)R * ns, st));
+        if (rc == FMM_OK) rc = presum(*d, A, lda, B, ldb, ps, ms, ns, ks, st);
+        if (rc == FMM_OK)
+          rc = launch_gemm(K_GEMM_FMM, d->prods_all, d->terms_all, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
+                           ps, C, ldc, nullptr, 0, 0, ms, ns, kp, st, true, ks);
+        cudaError_t fe = cudaFreeAsync(ws, st);
+        if (rc == FMM_OK) rc = cuda_status(fe);
+      } else if (use_presum(plan, ms, ns, ks)) {
         // U/V sums formed once per product in HBM (bandwidth-bound), then every
         // product reads single operands; products scattered into C in the epilogue.
         PresumOps ps;
@@ -884,6 +947,9 @@ int fmm_plan_destroy(fmm_plan* plan) {
     cudaFree(d.terms_ps);
     cudaFree(d.plistA);
     cudaFree(d.plistB);
+    cudaFree(d.prods_all);
+    cudaFree(d.terms_all);
+    cudaFree(d.plist_all);
   }
   delete plan;
   return FMM_OK;
