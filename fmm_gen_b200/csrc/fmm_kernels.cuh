@@ -1225,9 +1225,11 @@ __device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j, long l
   const int hr = (a.rows + 1) / 2;  // row pairs per column
   const long long total = lincomb_pairs(a);
   const long long e1 = min(total, (chunk + 1) * LINCOMB_CHUNK);
-  for (long long e = chunk * LINCOMB_CHUNK + threadIdx.x; e < e1; e += blockDim.x) {
-    const int i = 2 * (int)(e % hr);
-    const long long c = e / hr;
+  long long e = chunk * LINCOMB_CHUNK + threadIdx.x;
+  int ip = (int)(e % hr);  // row pair and column of element e, then stepped without division
+  long long c = e / hr;
+  for (; e < e1; e += blockDim.x) {
+    const int i = 2 * ip;
     const bool two = i + 1 < a.rows;
     double v0 = 0.0, v1 = 0.0;
     for (int t = 0; t < nt; ++t) {
@@ -1251,6 +1253,11 @@ __device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j, long l
     } else {
       o[0] = v0;
       if (two) o[1] = v1;
+    }
+    ip += blockDim.x;
+    while (ip >= hr) {
+      ip -= hr;
+      ++c;
     }
   }
 }
