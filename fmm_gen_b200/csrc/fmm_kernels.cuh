@@ -1232,20 +1232,36 @@ __device__ __forceinline__ void lincomb_body(const LincombArgs& a, int j, long l
     const int i = 2 * ip;
     const bool two = i + 1 < a.rows;
     double v0 = 0.0, v1 = 0.0;
-    for (int t = 0; t < nt; ++t) {
-      const Term tm = a.terms[t0 + t];
-      const double* x = a.X + (long long)tm.row * a.blk_row_stride + i + ((long long)tm.col * a.blk_col_stride + c) * a.ldx;
-      double x0, x1 = 0.0;
-      if (two && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
-        const double2 xx = *reinterpret_cast<const double2*>(x);
-        x0 = xx.x;
-        x1 = xx.y;
-      } else {
-        x0 = x[0];
-        if (two) x1 = x[1];
+    // terms in groups of four: the group's loads are issued before its fmas, so a thread
+    // keeps several loads in flight (the sum order is unchanged)
+    for (int tg = 0; tg < nt; tg += 4) {
+      double x0[4], x1[4], cf[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        x0[q] = x1[q] = cf[q] = 0.0;
+        if (tg + q < nt) {
+          const Term tm = a.terms[t0 + tg + q];
+          cf[q] = tm.coef;
+          const double* x =
+              a.X + (long long)tm.row * a.blk_row_stride + i + ((long long)tm.col * a.blk_col_stride + c) * a.ldx;
+          if (two && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+            const double2 xx = *reinterpret_cast<const double2*>(x);
+            x0[q] = xx.x;
+            x1[q] = xx.y;
+          } else {
+            x0[q] = x[0];
+            if (two) x1[q] = x[1];
+          }
+        }
       }
-      v0 = (t == 0) ? tm.coef * x0 : fma(tm.coef, x0, v0);
-      v1 = (t == 0) ? tm.coef * x1 : fma(tm.coef, x1, v1);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int t = tg + q;
+        if (t < nt) {
+          v0 = (t == 0) ? cf[q] * x0[q] : fma(cf[q], x0[q], v0);
+          v1 = (t == 0) ? cf[q] * x1[q] : fma(cf[q], x1[q], v1);
+        }
+      }
     }
     double* o = out + i + c * a.ldo;
     if (two && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
