@@ -38,9 +38,9 @@ UNIT = "TFLOP/s"
 CPU_SAMPLE = (14400, 14400, 480)
 # DRAM traffic of the FMM products launches per executed core flop, from a one-pass ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of one timed step of this workload:
-# 257.1 GB over 6.88e12 executed flops (16384^3: 180.9 GB, 14400x14400x480: 58.0 GB,
-# 4000x16000x2000: 18.2 GB), summarised in profiles/.
-TRAFFIC_BYTES_PER_FLOP = 257.1e9 / 6.88e12
+# 226.9 GB over 6.88e12 executed flops (16384^3: 153.9 GB, 14400x14400x480: 55.7 GB,
+# 4000x16000x2000: 17.3 GB), summarised in profiles/.
+TRAFFIC_BYTES_PER_FLOP = 226.9e9 / 6.88e12
 
 
 def effective_flops(shapes):
