@@ -270,3 +270,16 @@ def test_gpu_torch_custom_op(oracle_lib):
     want2 = C.copy(order="F")
     oracle_lib.bl_dgemm(A, B, want2)
     assert rel_fro(dC2.cpu().numpy(), want2) <= RTOL_SMALL
+
+
+@pytest.mark.parametrize("m,n,k", [(300, 200, 1), (129, 257, 5), (640, 384, 13), (1024, 1000, 1001), (77, 4100, 999)])
+def test_gpu_plain_k_tail(oracle_lib, m, n, k):
+    """The classical kernel with k not a multiple of its 8-deep k step: the last step reads
+    the tensor copies' zero fill past the operands' last column / row (direct staging)."""
+    A, B, C = inputs(m * 31 + n * 7 + k, m, n, k)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    rt.plain_gemm(dA, dB, dC)
+    got = dC.cpu().numpy()
+    want = C.copy(order="F")
+    oracle_lib.bl_dgemm(A, B, want)
+    assert rel_fro(got, want) <= RTOL_SMALL
