@@ -236,6 +236,39 @@ def split_bf16_8192(rt, torch, dev, steps=3):
     return out
 
 
+def strassen_2048(rt, torch, dev, steps=5):
+    """222-1 abc at 2048^3 (the minimum slice: A, B ~ U(-1,1), C = 0): effective TFLOPS beside
+    the plain kernel, and the relative error against an FP64 classical GEMM (cuBLAS)."""
+    n = 2048
+    g = torch.Generator(device=dev).manual_seed(2048)
+    A = rt.colmajor(n, n, device=dev).uniform_(-1, 1, generator=g)
+    B = rt.colmajor(n, n, device=dev).uniform_(-1, 1, generator=g)
+    C = rt.colmajor(n, n, device=dev).zero_()
+    p1 = rt.Plan.from_levels(["222"], [1])
+    rt.fmm_gemm(p1, A, B, C, "abc")
+    ref = A @ B
+    torch.cuda.synchronize()
+    err = ((C - ref).norm() / ref.norm()).item()
+
+    def t(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    f = 2.0 * n ** 3
+    ms_f = t(lambda: rt.fmm_gemm(p1, A, B, C, "abc"))
+    ms_p = t(lambda: rt.plain_gemm(A, B, C))
+    return {"algorithm": "222-1", "pack_type": "abc", "shape": [n, n, n], "ms": ms_f,
+            "tflops_effective": f / (ms_f * 1e-3) / 1e12, "plain_tflops": f / (ms_p * 1e-3) / 1e12,
+            "rel_fro_err_vs_cublas": err}
+
+
 def _measured_peak(key):
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -488,6 +521,7 @@ def main():
     if not args.no_extra:
         del mats
         torch.cuda.empty_cache()
+        extra["strassen_222_1_2048"] = strassen_2048(rt, torch, dev)
         extra["split_bf16_222_2_8192"] = split_bf16_8192(rt, torch, dev)
         extra["batch_512_fp64"] = batch_512(rt, torch, dev)
         del A16, B16, C16

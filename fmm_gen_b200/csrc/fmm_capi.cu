@@ -476,7 +476,7 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
   }
-  const bool direct = direct_ok && tma && mode == fmm::MODE_ACCUM_C && whole_k_steps(grid_dims, ks);
+  const bool direct = direct_ok && tma && whole_k_steps(grid_dims, ks);
   {
     ProfScope ps(kind, st);
     if (direct)
@@ -644,6 +644,66 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
   return cuda_status(cudaGetLastError());
 }
 
+// Pre-summed operands for the products of one call: the workspace, the operand sums and the
+// tables the products kernel reads them with.  When ks is not a multiple of the k step every
+// product gets its own slot whose k extent is padded with zeros (kk = ks rounded up), so all
+// k steps stay inside the slot and the direct variant can run.
+struct PresumPlan {
+  PresumOps ps;
+  const fmm::Prod* prods = nullptr;
+  const fmm::Term* terms = nullptr;
+  int kk = 0;
+  char* ws = nullptr;
+};
+
+int presum_prepare(const fmm_plan* plan, const DevTables& d, const double* A, long long lda, const double* B,
+                   long long ldb, int ms, int ns, int ks, cudaStream_t st, PresumPlan* out) {
+  const int R = plan->rank;
+  PresumOps& ps = out->ps;
+  int rc = FMM_OK;
+  if (ks % fmm::BK != 0) {
+    const int kp = (ks + fmm::BK - 1) / fmm::BK * fmm::BK;
+    ps.plistA = d.plist_all;
+    ps.plistB = d.plist_all;
+    ps.kslot = kp;
+    const size_t sbytes = sizeof(double) * (size_t)ms * kp * R;
+    const size_t tbytes = sizeof(double) * (size_t)kp * ns * R;
+    FMM_CUDA_TRY(cudaMallocAsync((void**)&out->ws, sbytes + tbytes + 16, st));
+    ps.S = reinterpret_cast<double*>(out->ws);
+    ps.ldS = ms;
+    ps.nslotA = R;
+    ps.T = reinterpret_cast<double*>(out->ws + sbytes);
+    ps.ldT = kp;
+    ps.nslotB = R;
+    // zero padding: S slot r columns [ks, kp); T rows [ks, kp) of every column
+    rc = cuda_status(cudaMemset2DAsync(out->ws + sizeof(double) * (size_t)ms * ks, sizeof(double) * (size_t)ms * kp,
+                                       0, sizeof(double) * (size_t)ms * (kp - ks), R, st));
+    if (rc == FMM_OK)
+      rc = cuda_status(cudaMemset2DAsync(out->ws + sbytes + sizeof(double) * ks, sizeof(double) * kp, 0,
+                                         sizeof(double) * (kp - ks), (size_t)R * ns, st));
+    out->prods = d.prods_all;
+    out->terms = d.terms_all;
+    out->kk = kp;
+  } else {
+    const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
+    const long long ldT = ks + (ks & 1);
+    const size_t sbytes = sizeof(double) * (size_t)ms * ks * nA;
+    const size_t tbytes = sizeof(double) * (size_t)ldT * ns * nB;
+    FMM_CUDA_TRY(cudaMallocAsync((void**)&out->ws, sbytes + tbytes + 16, st));
+    ps.S = reinterpret_cast<double*>(out->ws);
+    ps.ldS = ms;
+    ps.nslotA = nA;
+    ps.T = reinterpret_cast<double*>(out->ws + sbytes);
+    ps.ldT = ldT;
+    ps.nslotB = nB;
+    out->prods = d.prods_ps;
+    out->terms = d.terms_ps;
+    out->kk = ks;
+  }
+  if (rc == FMM_OK) rc = presum(d, A, lda, B, ldb, ps, ms, ns, ks, st);
+  return rc;
+}
+
 int check_args(int m, int n, int k, const void* A, long long lda, const void* B, long long ldb, const void* C,
                long long ldc) {
   if (m < 0 || n < 0 || k < 0) return FMM_E_INVALID;
@@ -670,57 +730,18 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
       const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
-      if (use_presum(plan, ms, ns, ks) && ks % fmm::BK != 0) {
-        // Every product pre-summed into slots whose k extent is padded with zeros to a
-        // multiple of the k step: all k steps are whole, so the direct variant runs.
-        const int kp = (ks + fmm::BK - 1) / fmm::BK * fmm::BK;
-        PresumOps ps;
-        ps.plistA = d->plist_all;
-        ps.plistB = d->plist_all;
-        ps.kslot = kp;
-        const size_t sbytes = sizeof(double) * (size_t)ms * kp * R;
-        const size_t tbytes = sizeof(double) * (size_t)kp * ns * R;
-        char* ws = nullptr;
-        FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, sbytes + tbytes + 16, st));
-        ps.S = reinterpret_cast<double*>(ws);
-        ps.ldS = ms;
-        ps.nslotA = R;
-        ps.T = reinterpret_cast<double*>(ws + sbytes);
-        ps.ldT = kp;
-        ps.nslotB = R;
-        // zero padding: S slot r columns [ks, kp); T rows [ks, kp) of every column
-        rc = cuda_status(cudaMemset2DAsync(ws + sizeof(double) * (size_t)ms * ks, sizeof(double) * (size_t)ms * kp, 0,
-                                           sizeof(double) * (size_t)ms * (kp - ks), R, st));
-        if (rc == FMM_OK)
-          rc = cuda_status(cudaMemset2DAsync(ws + sbytes + sizeof(double) * ks, sizeof(double) * kp, 0,
-                                             sizeof(double) * (kp - ks), (size_t)R * ns, st));
-        if (rc == FMM_OK) rc = presum(*d, A, lda, B, ldb, ps, ms, ns, ks, st);
-        if (rc == FMM_OK)
-          rc = launch_gemm(K_GEMM_FMM, d->prods_all, d->terms_all, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
-                           ps, C, ldc, nullptr, 0, 0, ms, ns, kp, st, true, ks);
-        cudaError_t fe = cudaFreeAsync(ws, st);
-        if (rc == FMM_OK) rc = cuda_status(fe);
-      } else if (use_presum(plan, ms, ns, ks)) {
+      if (use_presum(plan, ms, ns, ks)) {
         // U/V sums formed once per product in HBM (bandwidth-bound), then every
         // product reads single operands; products scattered into C in the epilogue.
-        PresumOps ps;
-        const long long ldT = ks + (ks & 1);
-        const size_t sbytes = sizeof(double) * (size_t)ms * ks * nA;
-        const size_t tbytes = sizeof(double) * (size_t)ldT * ns * nB;
-        char* ws = nullptr;
-        FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, sbytes + tbytes + 16, st));
-        ps.S = reinterpret_cast<double*>(ws);
-        ps.ldS = ms;
-        ps.nslotA = nA;
-        ps.T = reinterpret_cast<double*>(ws + sbytes);
-        ps.ldT = ldT;
-        ps.nslotB = nB;
-        rc = presum(*d, A, lda, B, ldb, ps, ms, ns, ks, st);
+        PresumPlan pp;
+        rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
         if (rc == FMM_OK)
-          rc = launch_gemm(K_GEMM_FMM, d->prods_ps, d->terms_ps, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
-                           ps, C, ldc, nullptr, 0, 0, ms, ns, ks, st, true);
-        cudaError_t fe = cudaFreeAsync(ws, st);
-        if (rc == FMM_OK) rc = cuda_status(fe);
+          rc = launch_gemm(K_GEMM_FMM, pp.prods, pp.terms, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, pp.ps,
+                           C, ldc, nullptr, 0, 0, ms, ns, pp.kk, st, true, ks);
+        if (pp.ws) {
+          cudaError_t fe = cudaFreeAsync(pp.ws, st);
+          if (rc == FMM_OK) rc = cuda_status(fe);
+        }
       } else {
         rc = launch_gemm(K_GEMM_FMM, d->prods, d->terms, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb,
                          PresumOps{}, C, ldc, nullptr, 0, 0, ms, ns, ks, st);
@@ -737,7 +758,19 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
       char* ws = nullptr;
       FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes + s_bytes + t_bytes, st));
       double* M = reinterpret_cast<double*>(ws);
-      if (pack == FMM_PACK_AB) {
+      if (pack == FMM_PACK_AB && use_presum(plan, ms, ns, ks)) {
+        // large sub-blocks: operands pre-summed as for ABC, each product stored to M by the
+        // direct variant, W applied by the combine pass below
+        PresumPlan pp;
+        rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
+        if (rc == FMM_OK)
+          rc = launch_gemm(K_GEMM_FMM, pp.prods, pp.terms, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb, pp.ps,
+                           C, ldc, M, ms, mstride, ms, ns, pp.kk, st, true, ks);
+        if (pp.ws) {
+          cudaError_t fe = cudaFreeAsync(pp.ws, st);
+          if (rc == FMM_OK) rc = cuda_status(fe);
+        }
+      } else if (pack == FMM_PACK_AB) {
         rc = launch_gemm(K_GEMM_FMM, d->prods, d->terms, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb,
                          PresumOps{}, C, ldc, M, ms, mstride, ms, ns, ks, st);
       } else {

@@ -1077,7 +1077,7 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
     for (int r = w.r0; r < w.r1; ++r, ++q) {
       const Prod p = a.prods[r];
       // the unit's C tiles into L2 while its product is still being computed
-      for (int c = 0; c < p.nc; ++c) {
+      for (int c = 0; a.mode == MODE_ACCUM_C && c < p.nc; ++c) {
         const Term tm = a.terms[p.c0 + c];
         const double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc;
         for (int l = et; l < (BM / 16) * BN; l += NEPI_D) {
@@ -1086,6 +1086,21 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
         }
       }
       mbar_wait(mfull, (unsigned)(q & 1), src.status());
+      if (a.mode == MODE_STORE_M) {  // the product tile to its workspace (the AB pack type)
+        double* Mr = a.M + (long long)r * a.m_stride + w.m0 + lane;
+        const int rmax = a.ms - w.m0 - lane;
+#pragma unroll 1
+        for (int col = ew; col < BN; col += NW) {
+          if (w.n0 + col >= a.ns) continue;
+          double* mp = Mr + (long long)(w.n0 + col) * a.ldm;
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch)
+            if (ch * 32 < rmax) mp[ch * 32] = Ms[col * MS_LD + lane + ch * 32];
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(mempty);
+        continue;
+      }
       if (ordered && r == w.r0) {
         if (et == 0) {
           const int* tp = a.tickets + w.tile;

@@ -38,7 +38,8 @@ extern "C" {
 #define FMM_E_TOO_LARGE (-8)    /* beyond the fixed limits of fmm_dgemm_dev_noalloc */
 
 #define FMM_PACK_ABC 0    /* sums fused into operand staging, products scattered into C */
-#define FMM_PACK_AB 1     /* sums fused into staging, each product to a workspace M_r, then scatter */
+#define FMM_PACK_AB 1     /* each product to a workspace M_r, then M_Add (sums fused into staging,
+                             or pre-summed in HBM for large sub-blocks) */
 #define FMM_PACK_NAIVE 2  /* explicit S_r, T_r temporaries, plain GEMM into M_r, then scatter */
 
 typedef struct fmm_plan fmm_plan;
