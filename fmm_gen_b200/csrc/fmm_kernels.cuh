@@ -19,7 +19,12 @@
 //        (bounded spin, error flag on timeout), so no two CTAs ever update the same C
 //        element at once and products are applied in order r = 0..R-1.
 //   * M_Add / S_Add / T_Add (meta/ab_gen_mix.py:341-372, meta/naive_gen_mix.py:60-137)
-//     -> fmm_scatter_kernel / fmm_lincomb_kernel.
+//     -> fmm_lincomb_kernel / fmm_lincomb_batch_kernel (operand sums formed in HBM, also
+//        used by the ABC pack type for large sub-blocks), fmm_combine_kernel (every
+//        C_l += W[l,r] M_r of a batch of products in one pass), fmm_scatter_kernel.
+//   * The direct variant (fmm_gemm_direct_kernel) runs when every operand is a single
+//     aligned term (pre-summed operands): a deeper TMA pipeline and an epilogue on the
+//     producer warps that overlaps the next product's DMMA.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -529,7 +534,7 @@ __device__ __forceinline__ void producer(const Src& src, double* stages, double*
 // ------------------------------------------------------------------------------------
 // TMA producer.  Warp 0, lane 0 is the issuer: per k step it copies single-term
 // operands (coefficient 1, full k step, aligned) straight into the operand stage and
-// every term of a summed operand into a raw slot.  Warps 1..3 fold the raw slots of a
+// every term of a summed operand into a raw slot.  Warps 1..7 fold the raw slots of a
 // k step into registers (sum with coefficients, k tail masked) and store the result
 // into the stage once.  The stage's full barrier completes on the issuer's arrival
 // with its byte count plus one arrival per folding warp.
