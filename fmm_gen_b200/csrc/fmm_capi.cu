@@ -591,12 +591,13 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
 
 // Pre-summing pays off once the sub-blocks are large enough that the extra pass over HBM
 // (each operand sum written once, then read by every tile that uses it) costs less than
-// folding the sums while staging, which limits the producer warps.  Measured on B200:
-// 14400 x 14400 x 480 (k = 80 or 240 per product) 222-1 x 333-1 22.5 -> 19.1 ms, 222-1
-// 10.7 -> 7.8 ms with pre-sums; shapes with larger k unchanged.
+// folding the sums while staging, which limits the producer warps, and it lets the
+// direct kernel variant run.  Measured on B200 (pre-summed vs folded): 222-1 x 333-1
+// 4096^3 11.7 -> 5.4 ms, 4000 x 3840 x 2000 5.6 -> 3.3 ms, 14400 x 14400 x 480 22.5 ->
+// 19.1 ms; 222-2 2048^3 1.34 -> 0.88 ms; 222-1 1024^3 0.24 -> 0.17 ms (ms * ns = 2^18).
 bool use_presum(const fmm_plan* plan, int ms, int ns, int ks) {
   if (plan->plistA.empty() && plan->plistB.empty()) return false;
-  return (long long)ms * ns >= (1LL << 20) && ks >= 64;
+  return (long long)ms * ns >= (1LL << 17) && ks >= 64;
 }
 
 int presum(const DevTables& d, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
@@ -867,6 +868,35 @@ int device_status(bool clear) {
 }
 
 // Host-pointer execution: stage A, B, C into device memory, run, copy C back.
+//
+// Large problems run as column panels C[:, J] += A * B[:, J], each a GEMM of its own
+// (partitioned like any m x |J| x k call), so that the copies overlap the compute: A goes
+// in first, then panel j computes on the calling thread's stream while panel j+1's B and
+// C come in on one copy stream and panel j-1's C goes back on another (host-to-device and
+// device-to-host copies run at the same time).  With P panels only A plus one panel's B
+// and C are copied before the first kernel, and one panel's C after the last.  Panel
+// edges fall on multiples of 128 x (block columns of the plan), so every panel's
+// sub-blocks are whole 128-column tiles where the width allows.
+#ifndef FMM_HOST_PANELS
+#define FMM_HOST_PANELS 4
+#endif
+constexpr int kHostPanelMinCols = 2048;              // panels at least this wide
+constexpr long long kHostPanelMinElems = 1LL << 22;  // C of at least 32 MB
+
+int host_panels(const fmm_plan* plan, bool plain, int m, int n, std::vector<int>* edges) {
+  int P = 1;
+  if ((long long)m * n >= kHostPanelMinElems) P = std::max(1, std::min(FMM_HOST_PANELS, n / kHostPanelMinCols));
+  const int unit = 128 * ((plain || !plan) ? 1 : plan->dims[2]);
+  edges->assign(1, 0);
+  for (int j = 1; j < P; ++j) {
+    long long e = (long long)n * j / P;
+    if (n / P >= unit) e -= e % unit;
+    if (e > edges->back() && e < n) edges->push_back((int)e);
+  }
+  edges->push_back(n);
+  return (int)edges->size() - 1;
+}
+
 int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, const double* A, int lda,
              const double* B, int ldb, double* C, int ldc) {
   int rc = check_args(m, n, k, A, lda, B, ldb, C, ldc);
@@ -874,32 +904,63 @@ int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, co
   if (m == 0 || n == 0 || k == 0) return FMM_OK;
   if (!plain && !plan) return FMM_E_NOPLAN;
   cudaStream_t st = cudaStreamPerThread;
-  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
   // even device pitches for A and B: tensor copies need 16-byte column starts
   const int pa = m + (m & 1), pb = k + (k & 1);
   const size_t szA = sizeof(double) * (size_t)pa * k, szB = sizeof(double) * (size_t)pb * n,
                szC = sizeof(double) * (size_t)m * n;
-  FMM_CUDA_TRY(cudaMallocAsync((void**)&dA, szA, st));
-  FMM_CUDA_TRY(cudaMallocAsync((void**)&dB, szB, st));
-  FMM_CUDA_TRY(cudaMallocAsync((void**)&dC, szC, st));
-  FMM_CUDA_TRY(cudaMemcpy2DAsync(dA, sizeof(double) * pa, A, sizeof(double) * lda, sizeof(double) * m, k,
-                                 cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpy2DAsync(dB, sizeof(double) * pb, B, sizeof(double) * ldb, sizeof(double) * k, n,
-                                 cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpy2DAsync(dC, sizeof(double) * m, C, sizeof(double) * ldc, sizeof(double) * m, n,
-                                 cudaMemcpyHostToDevice, st));
-  if (plain)
-    rc = plain_gemm(m, n, k, dA, pa, dB, pb, dC, m, st);
-  else
-    rc = run_fmm(plan, pack, m, n, k, dA, pa, dB, pb, dC, m, st);
+  std::vector<int> edges;
+  const int P = host_panels(plan, plain, m, n, &edges);
+  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  cudaStream_t sin = nullptr, sout = nullptr;
+  std::vector<cudaEvent_t> ev;  // [0]: allocations made; [1 + j]: panel j copied in; [1 + P + j]: panel j done
+  auto ok = [&](cudaError_t e) {
+    if (rc == FMM_OK && e != cudaSuccess) rc = cuda_status(e);
+    return rc == FMM_OK;
+  };
+  ok(cudaMallocAsync((void**)&dA, szA, st)) && ok(cudaMallocAsync((void**)&dB, szB, st)) &&
+      ok(cudaMallocAsync((void**)&dC, szC, st));
+  if (rc == FMM_OK && P > 1) {
+    ok(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking)) &&
+        ok(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking));
+    ev.assign(1 + 2 * P, nullptr);
+    for (auto& e : ev)
+      if (!ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) break;
+  }
+  cudaStream_t cin = P > 1 ? sin : st, cout = P > 1 ? sout : st;
+  if (rc == FMM_OK && P > 1) ok(cudaEventRecord(ev[0], st)) && ok(cudaStreamWaitEvent(sin, ev[0], 0));
   if (rc == FMM_OK)
-    rc = cuda_status(cudaMemcpy2DAsync(C, sizeof(double) * ldc, dC, sizeof(double) * m, sizeof(double) * m, n,
-                                       cudaMemcpyDeviceToHost, st));
-  cudaFreeAsync(dA, st);
-  cudaFreeAsync(dB, st);
-  cudaFreeAsync(dC, st);
-  cudaError_t se = cudaStreamSynchronize(st);
-  if (rc == FMM_OK) rc = cuda_status(se);
+    ok(cudaMemcpy2DAsync(dA, sizeof(double) * pa, A, sizeof(double) * lda, sizeof(double) * m, k,
+                         cudaMemcpyHostToDevice, cin));
+  for (int j = 0; j < P && rc == FMM_OK; ++j) {
+    const int c0 = edges[j], nj = edges[j + 1] - edges[j];
+    ok(cudaMemcpy2DAsync(dB + (size_t)c0 * pb, sizeof(double) * pb, B + (size_t)c0 * ldb, sizeof(double) * ldb,
+                         sizeof(double) * k, nj, cudaMemcpyHostToDevice, cin)) &&
+        ok(cudaMemcpy2DAsync(dC + (size_t)c0 * m, sizeof(double) * m, C + (size_t)c0 * ldc, sizeof(double) * ldc,
+                             sizeof(double) * m, nj, cudaMemcpyHostToDevice, cin));
+    if (P > 1 && rc == FMM_OK) ok(cudaEventRecord(ev[1 + j], sin));
+  }
+  for (int j = 0; j < P && rc == FMM_OK; ++j) {
+    const int c0 = edges[j], nj = edges[j + 1] - edges[j];
+    if (P > 1 && !ok(cudaStreamWaitEvent(st, ev[1 + j], 0))) break;
+    rc = plain ? plain_gemm(m, nj, k, dA, pa, dB + (size_t)c0 * pb, pb, dC + (size_t)c0 * m, m, st)
+               : run_fmm(plan, pack, m, nj, k, dA, pa, dB + (size_t)c0 * pb, pb, dC + (size_t)c0 * m, m, st);
+    if (rc != FMM_OK) break;
+    if (P > 1) ok(cudaEventRecord(ev[1 + P + j], st)) && ok(cudaStreamWaitEvent(sout, ev[1 + P + j], 0));
+    if (rc == FMM_OK)
+      ok(cudaMemcpy2DAsync(C + (size_t)c0 * ldc, sizeof(double) * ldc, dC + (size_t)c0 * m, sizeof(double) * m,
+                           sizeof(double) * m, nj, cudaMemcpyDeviceToHost, cout));
+  }
+  // join: every copy has finished before the buffers go back to the pool
+  if (sin) ok(cudaStreamSynchronize(sin));
+  if (sout) ok(cudaStreamSynchronize(sout));
+  if (dA) cudaFreeAsync(dA, st);
+  if (dB) cudaFreeAsync(dB, st);
+  if (dC) cudaFreeAsync(dC, st);
+  ok(cudaStreamSynchronize(st));
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
+  if (sin) cudaStreamDestroy(sin);
+  if (sout) cudaStreamDestroy(sout);
   if (rc == FMM_OK) rc = device_status(true);
   return rc;
 }

@@ -728,27 +728,80 @@ __device__ __forceinline__ void tma_folder(const Src& src, double* stages, const
 
 // ------------------------------------------------------------------------------------
 // Consumers: DMMA over the stages, then the multi-destination epilogue.
+//
+// Consumer warp (wm, wn) owns tile rows wm*64 + 16i + 0..15 and tile columns
+// frag_col(wn, j) + 0..7 for fragments i, j = 0..3.  The columns are interleaved (warp wn
+// owns wn*8 + 32j) so that a tile cut short by the block edge still spreads its column
+// fragments over all four warps of a row half; with the warp-to-scheduler mapping (warp
+// % 4, i.e. wn) every SM sub-partition then skips about the same share of an edge tile.
 // ------------------------------------------------------------------------------------
-__device__ __forceinline__ void mma_stage(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
-                                          int wn, int g, int t4) {
+__device__ __forceinline__ int frag_col(int wn, int j) { return wn * 8 + j * 32; }
+
+// Fragments of warp (wm, wn) that hold rows < vr and columns < vc of the tile: i < im, j < jn.
+__device__ __forceinline__ void frag_counts(int vr, int vc, int wm, int wn, int& im, int& jn) {
+  const int rrem = vr - wm * 64, crem = vc - wn * 8;
+  im = rrem <= 0 ? 0 : min(4, (rrem + 15) >> 4);
+  jn = crem <= 0 ? 0 : min(4, (crem + 31) >> 5);
+}
+
+// One operand stage into the fragments i < IM, j < JN of the accumulator (IM = JN = 4:
+// the whole 64 x 32 warp tile; fewer for the warps of an edge tile, whose other
+// fragments stay as they were and are never written out).  Compile-time counts keep each
+// form straight-line code: shared-memory loads and DMMAs with no predicates.
+template <int IM, int JN>
+__device__ __forceinline__ void mma_stage_t(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
+                                            int wn, int g, int t4) {
 #pragma unroll
   for (int kq = 0; kq < BK / 4; ++kq) {
     double af[4][2], bf[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < IM; ++i) {
       const int row = wm * 64 + i * 16 + g;
       af[i][0] = opA[(kq * 4 + t4) * LDA_S + row];
       af[i][1] = opA[(kq * 4 + t4) * LDA_S + row + 8];
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int col = wn * 32 + j * 8 + g;
-      bf[j] = opB[col * LDB_S + kq * 4 + t4];
+    for (int j = 0; j < JN; ++j) bf[j] = opB[(frag_col(wn, j) + g) * LDB_S + kq * 4 + t4];
+#pragma unroll
+    for (int i = 0; i < IM; ++i)
+#pragma unroll
+      for (int j = 0; j < JN; ++j) dmma_16x8x4(acc[i][j], af[i], bf[j]);
+  }
+}
+
+template <int IM_, int JN_>
+struct Frags {
+  static constexpr int IM = IM_, JN = JN_;
+};
+
+// Calls f(Frags<IM, JN>{}) with IM >= im, JN >= jn, so that a k loop written once is
+// compiled for the edge shapes: full tiles (4, 4), bottom-edge (1..3, 4), right-edge
+// (4, 1..3) and idle warps (0, 0); a corner takes the cheaper of its two edge forms.
+// Extra fragments are harmless, and eight forms instead of all seventeen keep the
+// consumer code small: on B200 the full set cost 1.5 % on short-k shapes.
+template <class F>
+__device__ __forceinline__ void with_frags(int im, int jn, F&& f) {
+  if (im == 4 && jn == 4) {
+    f(Frags<4, 4>{});
+    return;
+  }
+  if (im <= 0 || jn <= 0) {
+    f(Frags<0, 0>{});
+    return;
+  }
+  if (jn < 4 && (im == 4 || jn < im)) {
+    switch (jn) {
+      case 1: f(Frags<4, 1>{}); break;
+      case 2: f(Frags<4, 2>{}); break;
+      default: f(Frags<4, 3>{}); break;
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) dmma_16x8x4(acc[i][j], af[i], bf[j]);
+    return;
+  }
+  switch (im) {
+    case 1: f(Frags<1, 4>{}); break;
+    case 2: f(Frags<2, 4>{}); break;
+    case 3: f(Frags<3, 4>{}); break;
+    default: f(Frags<4, 4>{}); break;
   }
 }
 
@@ -765,7 +818,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
-            const int cc = n0 + wn * 32 + j * 8 + t4 * 2 + q;
+            const int cc = n0 + frag_col(wn, j) + t4 * 2 + q;
             if (rr < a.ms && cc < a.ns) Mr[rr + (long long)cc * a.ldm] = acc[i][j][2 * h + q];
           }
     return;
@@ -789,7 +842,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
               const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
-              const int cc = n0 + wn * 32 + (jb + j) * 8 + t4 * 2 + q;
+              const int cc = n0 + frag_col(wn, jb + j) + t4 * 2 + q;
               cv[j][2 * h + q] = (rr < a.ms && cc < a.ns) ? Cb[rr + (long long)cc * a.ldc] : 0.0;
             }
 #pragma unroll
@@ -799,7 +852,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, const Prod& p, int r
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
               const int rr = m0 + wm * 64 + i * 16 + g + 8 * h;
-              const int cc = n0 + wn * 32 + (jb + j) * 8 + t4 * 2 + q;
+              const int cc = n0 + frag_col(wn, jb + j) + t4 * 2 + q;
               if (rr < a.ms && cc < a.ns)
                 Cb[rr + (long long)cc * a.ldc] = fma(w, acc[i][jb + j][2 * h + q], cv[j][2 * h + q]);
             }
@@ -883,7 +936,7 @@ __device__ __forceinline__ void consumer(const Src& src, const double* stages, u
         const double* opB = opA + OPA_SZ;
         mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE) & 1), src.status());
         if (s == (nks > C_PREFETCH_STEPS ? nks - C_PREFETCH_STEPS : 0)) prefetch_c_tiles(a, p, w.m0, w.n0, ct);
-        mma_stage(opA, opB, acc, wm, wn, g, t4);
+        mma_stage_t<4, 4>(opA, opB, acc, wm, wn, g, t4);
         // The stage is refilled by TMA as soon as every warp has arrived; the fence
         // makes this warp's shared-memory fragment loads complete before its arrival
         // (measured: without it a refill could overwrite fragments still in flight).
@@ -1024,6 +1077,8 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
     const GemmArgs& a = src.get(job);
     const int nks = (a.ks + BK - 1) / BK;
     const Unit w = decode_unit(a, u - src.first_unit(job));
+    int im, jn;
+    frag_counts(a.ms - w.m0, a.ns - w.n0, wm, wn, im, jn);
 #pragma unroll 1
     for (int r = w.r0; r < w.r1; ++r, ++q) {
 #pragma unroll
@@ -1032,16 +1087,19 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
         for (int j = 0; j < 4; ++j)
 #pragma unroll
           for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+      with_frags(im, jn, [&](auto fr) {
+        using FR = decltype(fr);
 #pragma unroll 1
-      for (int s = 0; s < nks; ++s, ++kc) {
-        const int stage = (int)(kc % NSTAGE_D);
-        const double* opA = stages + (size_t)stage * STAGE_SZ;
-        mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
-        mma_stage(opA, opA + OPA_SZ, acc, wm, wn, g, t4);
-        __threadfence_block();  // fragment loads complete before the stage can be refilled
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty0 + 8 * stage);
-      }
+        for (int s = 0; s < nks; ++s, ++kc) {
+          const int stage = (int)(kc % NSTAGE_D);
+          const double* opA = stages + (size_t)stage * STAGE_SZ;
+          mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
+          mma_stage_t<FR::IM, FR::JN>(opA, opA + OPA_SZ, acc, wm, wn, g, t4);
+          __threadfence_block();  // fragment loads complete before the stage can be refilled
+          __syncwarp();
+          if (lane == 0) mbar_arrive(empty0 + 8 * stage);
+        }
+      });
       // hand the product tile to the epilogue warps once they are done with the previous one
       mbar_wait(mempty, (unsigned)((q & 1) ^ 1), src.status());
 #pragma unroll
@@ -1053,7 +1111,7 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int rr = wm * 64 + i * 16 + g + 8 * h;
-              const int cc = wn * 32 + j * 8 + t4 * 2 + e;
+              const int cc = frag_col(wn, j) + t4 * 2 + e;
               Ms[cc * MS_LD + rr] = acc[i][j][2 * h + e];
             }
       __syncwarp();

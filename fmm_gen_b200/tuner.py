@@ -91,7 +91,7 @@ def model_counts(plan: algebra.FMMPlan) -> List[int]:
 
 def _presummed(plan: algebra.FMMPlan, ms: int, ns: int, ks: int) -> bool:
     """The library's rule for forming operand sums in HBM before the products."""
-    return plan.rank > 1 and ms * ns >= (1 << 20) and ks >= 64
+    return plan.rank > 1 and ms * ns >= (1 << 17) and ks >= 64
 
 
 def _tiles(ms: int, ns: int) -> int:
