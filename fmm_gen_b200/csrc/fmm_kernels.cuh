@@ -102,7 +102,8 @@ struct Term {
   int col;      // global block column
   double coef;  // coefficient
   int src;      // A/B terms: 0 = the operand matrix, 1 = the pre-summed workspace (S / T)
-  int pad;
+  int pad;      // C terms: this product's position among the products with a term in the
+                // same C block (product order); the per-block tickets count up to it
 };
 
 struct Prod {
@@ -144,6 +145,9 @@ struct GemmArgs {
   int mode;
   int* tickets;     // per tile: chunks completed (zeroed before launch); used when chunks > 1
   unsigned* status; // device status word (StatusBits)
+  int nbt;          // > 0 (direct variant, one product per unit): tickets per (tile, C block),
+  int nbc;          // nbt = C blocks, index tile * nbt + row * nbc + col, counting the block's
+                    // updates in product order; 0: one ticket per tile
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -1164,7 +1168,8 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
         if (lane == 0) mbar_arrive(mempty);
         continue;
       }
-      if (ordered && r == w.r0) {
+      const bool per_block = ordered && a.nbt > 0;
+      if (ordered && !per_block && r == w.r0) {
         if (et == 0) {
           const int* tp = a.tickets + w.tile;
           if (ld_acquire(tp) < chunk) {
@@ -1188,6 +1193,22 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
       for (int c = 0; c < p.nc; ++c) {
         const Term tm = a.terms[p.c0 + c];
         const double wgt = tm.coef;
+        int* tk = nullptr;
+        if (per_block) {  // wait for the previous product that updates this C block
+          tk = a.tickets + (long long)w.tile * a.nbt + tm.row * a.nbc + tm.col;
+          if (et == 0 && ld_acquire(tk) < tm.pad) {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire(tk) < tm.pad) {
+              if (*(volatile unsigned*)a.status != 0u) break;
+              if (global_ns() - t0 > WAIT_LIMIT_NS) {
+                atomicOr(a.status, STATUS_TICKET_TIMEOUT);
+                break;
+              }
+              __nanosleep(128);
+            }
+          }
+          named_bar_sync(2, NEPI_D);
+        }
         double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc + w.m0 + lane;
         const int rmax = a.ms - w.m0 - lane;  // rows of this lane inside the block: rr < rmax
 #pragma unroll 1
@@ -1212,11 +1233,16 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
               if (ch * 32 < rmax) cp[ch * 32] = fma(wgt, mp[ch * 32], cv[cb][ch]);
           }
         }
+        if (tk) {  // this block's update is visible before the next product may start its own
+          __threadfence();
+          named_bar_sync(2, NEPI_D);
+          if (et == 0) st_release(tk, tm.pad + 1);
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(mempty);  // the buffer can take the next product
     }
-    if (ordered) {
+    if (ordered && a.nbt == 0) {
       __threadfence();
       named_bar_sync(2, NEPI_D);
       if (et == 0) st_release(a.tickets + w.tile, chunk + 1);
