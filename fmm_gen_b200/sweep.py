@@ -14,7 +14,8 @@ by eye (meta/model_gen.py:132-175).  The same families here, in one process:
         --out square.csv
 
 One row per (size, algorithm): effective GFLOPS of the FMM (ABC), of the classical kernel, the
-B200 model's prediction for both, and the relative difference between the two results.
+B200 model's single-problem prediction for both (tuner.model_time_single), and the relative
+difference between the two results.
 """
 from __future__ import annotations
 
@@ -39,7 +40,7 @@ def shapes(family: str, sizes: Iterable[int]) -> List[Tuple[int, int, int]]:
 
 
 def model_gflops(alg: str, m: int, n: int, k: int, model: tuner.B200Model) -> float:
-    return 2.0 * m * n * k / tuner.model_time(model, alg, m, n, k) / 1e9
+    return 2.0 * m * n * k / tuner.model_time_single(model, alg, m, n, k) / 1e9
 
 
 HEADER = ["family", "algorithm", "m", "n", "k", "gflops_fmm", "gflops_gemm", "model_gflops_fmm",

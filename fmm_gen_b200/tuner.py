@@ -7,17 +7,23 @@ time = actual_flops * tau + memops * alpha for its CPU blocking MC/KC/NC).  The 
 structure is re-derived here for this implementation on B200:
 
   * compute: every product of a job is a sub-GEMM tiled 128 x 128 with k steps of 8.
-    A k step costs `kstep_s` on one SM at the plain kernel's rate; a product whose
-    operand sums are folded while staging costs `1 + fold_per_term * (T - 1)` times
-    that (T = the larger of its A and B term counts); pre-summed products cost 1.
+    A k step costs `kstep_s` on one SM at the plain kernel's rate.  A product whose
+    operand sums are folded while staging costs `1 + fold_per_term * (T - 1)` times that
+    (T = the larger of its A and B term counts) on whole tiles; pre-summed products (and
+    classical jobs) run in the direct kernel variant, cost 1, and their edge tiles count
+    only the 16-row / 32-column fragments they compute.
   * memory: the pre-sum pass reads every U/V term and writes each summed operand once
-    (HBM bytes / bandwidth, a separate pass), and the multi-destination epilogue reads
-    and writes one C tile per W nonzero, counted `c_exposed` times its HBM time (it does
-    not overlap the MMAs; fitted to measurements).
+    (HBM bytes / bandwidth, a separate pass).  The multi-destination epilogue reads and
+    writes one C tile per W nonzero: in the direct variant it overlaps the products'
+    MMAs (the job takes the longer of the two, the C traffic counted `c_direct` times its
+    HBM time); in the folded kernel it does not (`c_exposed` times, added).
   * partition: the same fringe split as the library (algebra.partition); the strips
     are classical jobs.
-Time is in the batch's throughput view: SM-seconds / SMs plus the exposed memory time
-(a batch keeps every SM busy, so wave quantisation of a single problem does not apply).
+`model_time` is the batch's throughput view: SM-seconds / SMs plus the exposed memory
+time (a batch keeps every SM busy, so wave quantisation of a single problem does not
+apply).  `model_time_single` is one problem on its own: every launch (pre-sum pass, FMM
+products, each fringe strip) takes whole waves of work units over the SMs plus a launch
+latency.
 
 The tuner takes the model's best candidate per problem, then measures the whole batch
 and re-assigns groups of problems (by the model's choice and margin) while that makes the
@@ -41,19 +47,24 @@ KSTEP = 8
 
 @dataclass
 class B200Model:
-    """Constants of the model; defaults are this implementation's measurements on B200:
+    """Constants of the model; defaults are this implementation's measurements on B200.
+
     plain FP64 kernel 34.5 TFLOP/s; folded 222-1 products at 1.7x a plain k step; 6.5 TB/s
-    copy bandwidth; and `c_exposed` fitted to the sweep runner's measurements (square
-    4096-16384, rank-k 14400^2 x 480-7680, fixed-k 1024; 222-1, 222-2, 222-1 x 333-1, 39
-    points): the multi-destination C epilogue is not hidden under the MMAs (1.5 x its HBM
-    time), which brings the model within 3.4 % RMS of the measured FMM rates (0.3 gave 21 %)."""
+    copy bandwidth; `c_exposed` fitted to the folded kernel (the epilogue on the consumer
+    warps, 1.5 x its HBM time); `c_direct`, `wave_unit_s` and `launch_s` fitted to 17
+    single-problem measurements of the direct variant (222-1, 222-2, 222-1 x 333-1 and
+    classical, 1024^3 to 16384^3 and the rank-k shapes): `model_time_single` is within
+    9 % RMS (log ratio) of them, 3-5 % on the large shapes."""
 
     sms: int = 148
     plain_tflops: float = 34.5
     hbm_gbs: float = 6500.0
     fold_per_term: float = 0.7
     c_exposed: float = 1.5
-    unit_overhead_s: float = 1.5e-6  # pipeline fill + epilogue latency per work unit
+    c_direct: float = 1.6
+    unit_overhead_s: float = 1.5e-6  # pipeline fill + epilogue latency per work unit (batch view)
+    wave_unit_s: float = 8e-6        # the same seen by one problem (its last epilogue is exposed)
+    launch_s: float = 20e-6          # per launch of one problem
 
     @property
     def kstep_s(self) -> float:
@@ -98,51 +109,108 @@ def _tiles(ms: int, ns: int) -> int:
     return math.ceil(ms / TILE) * math.ceil(ns / TILE)
 
 
+def _tile_work(ms: int, ns: int) -> float:
+    """Tiles of an ms x ns sub-block in the direct variant, an edge tile counted by the
+    fragments it computes: 16-row fragments at the bottom edge, 32-column groups at the
+    right edge, the cheaper of the two at the corner."""
+    fr, rr = divmod(ms, TILE)
+    fc, rc = divmod(ns, TILE)
+    rf = math.ceil(rr / 16) / 8 if rr else 0.0
+    cf = math.ceil(rc / 32) / 4 if rc else 0.0
+    return fr * fc + fc * rf + fr * cf + (min(rf, cf) if rr and rc else 0.0)
+
+
 def _classical_job(model: B200Model, m: int, n: int, k: int) -> Tuple[float, float, int]:
     if m <= 0 or n <= 0 or k <= 0:
         return 0.0, 0.0, 0
-    t = _tiles(m, n)
-    return t * math.ceil(k / KSTEP) * model.kstep_s, 0.0, t
+    return _tile_work(m, n) * math.ceil(k / KSTEP) * model.kstep_s, 0.0, _tiles(m, n)
+
+
+def _core(model: B200Model, plan: algebra.FMMPlan, p) -> Dict[str, float]:
+    """The FMM products of one problem: SM-seconds, work units, pre-sum seconds, C epilogue
+    seconds and whether the epilogue overlaps the MMAs."""
+    tiles = _tiles(p.ms, p.ns)
+    ksteps = math.ceil(p.ks / KSTEP)
+    nu = np.count_nonzero(plan.U, axis=0)
+    nv = np.count_nonzero(plan.V, axis=0)
+    c_s = 16.0 * int(np.count_nonzero(plan.W)) * p.ms * p.ns / (model.hbm_gbs * 1e9)
+    if _presummed(plan, p.ms, p.ns, p.ks):
+        na, nb = int((nu > 1).sum()), int((nv > 1).sum())
+        bytes_ = 8.0 * (nu[nu > 1].sum() * p.ms * p.ks + na * p.ms * p.ks +
+                        nv[nv > 1].sum() * p.ks * p.ns + nb * p.ks * p.ns)
+        return {"sm_s": _tile_work(p.ms, p.ns) * ksteps * model.kstep_s * plan.rank, "units": tiles * plan.rank,
+                "presum_s": bytes_ / (model.hbm_gbs * 1e9), "c_s": model.c_direct * c_s, "overlap": True}
+    T = np.maximum(nu, nv)
+    factor = float((1.0 + model.fold_per_term * (T - 1)).sum())
+    return {"sm_s": tiles * ksteps * model.kstep_s * factor, "units": tiles * plan.rank, "presum_s": 0.0,
+            "c_s": model.c_exposed * c_s, "overlap": False}
+
+
+def _strips(p, m: int, n: int, k: int):
+    return ((p.md, p.nd, p.kr), (m, p.nr, k), (p.mr, p.nd, k))
 
 
 def job_costs(model: B200Model, name: str, m: int, n: int, k: int) -> Dict[str, float]:
-    """Modelled SM-seconds, exposed HBM seconds and work units of one problem."""
+    """Modelled SM-seconds, exposed HBM seconds (`mem_s`), HBM seconds that overlap the
+    MMAs (`ovl_s`) and work units of one problem."""
     plan = plan_of(name)
     if plan is None:
         sm, mem, units = _classical_job(model, m, n, k)
-        return {"sm_s": sm, "mem_s": mem, "units": units}
+        return {"sm_s": sm + units * model.unit_overhead_s, "mem_s": mem, "ovl_s": 0.0, "units": units}
     p = algebra.partition(m, n, k, plan.dims)
-    sm = mem = 0.0
+    sm = mem = ovl = 0.0
     units = 0
     if p.ms > 0 and p.ns > 0 and p.ks > 0:
-        tiles = _tiles(p.ms, p.ns)
-        ksteps = math.ceil(p.ks / KSTEP)
-        nu = np.count_nonzero(plan.U, axis=0)
-        nv = np.count_nonzero(plan.V, axis=0)
-        if _presummed(plan, p.ms, p.ns, p.ks):
-            factor = float(plan.rank)
-            na, nb = int((nu > 1).sum()), int((nv > 1).sum())
-            bytes_ = 8.0 * (nu[nu > 1].sum() * p.ms * p.ks + na * p.ms * p.ks +
-                            nv[nv > 1].sum() * p.ks * p.ns + nb * p.ks * p.ns)
-            mem += bytes_ / (model.hbm_gbs * 1e9)
+        c = _core(model, plan, p)
+        sm += c["sm_s"]
+        units += c["units"]
+        mem += c["presum_s"]
+        if c["overlap"]:
+            ovl += c["c_s"]
         else:
-            T = np.maximum(nu, nv)
-            factor = float((1.0 + model.fold_per_term * (T - 1)).sum())
-        sm += tiles * ksteps * model.kstep_s * factor
-        nnz_w = int(np.count_nonzero(plan.W))
-        mem += model.c_exposed * 16.0 * nnz_w * p.ms * p.ns / (model.hbm_gbs * 1e9)
-        units += tiles * max(1, min(plan.rank, math.ceil(plan.rank * ksteps / 512)))
-    for (mm, nn, kk) in ((p.md, p.nd, p.kr), (m, p.nr, k), (p.mr, p.nd, k)):
+            mem += c["c_s"]
+    for (mm, nn, kk) in _strips(p, m, n, k):
         s2, _, u2 = _classical_job(model, mm, nn, kk)
         sm += s2
         units += u2
     sm += units * model.unit_overhead_s
-    return {"sm_s": sm, "mem_s": mem, "units": units}
+    return {"sm_s": sm, "mem_s": mem, "ovl_s": ovl, "units": units}
 
 
 def model_time(model: B200Model, name: str, m: int, n: int, k: int) -> float:
+    """Throughput view (one problem of a batch that keeps every SM busy)."""
     c = job_costs(model, name, m, n, k)
-    return c["sm_s"] / model.sms + c["mem_s"]
+    return max(c["sm_s"] / model.sms, c["ovl_s"]) + c["mem_s"]
+
+
+def model_time_single(model: B200Model, name: str, m: int, n: int, k: int) -> float:
+    """One problem on its own: whole waves of work units per launch plus launch latency."""
+
+    def launch(sm_s: float, units: int) -> float:
+        if units <= 0:
+            return 0.0
+        return math.ceil(units / model.sms) * (sm_s / units + model.wave_unit_s) + model.launch_s
+
+    def classical(mm: int, nn: int, kk: int) -> float:
+        s, _, u = _classical_job(model, mm, nn, kk)
+        return launch(s, u)
+
+    plan = plan_of(name)
+    if plan is None:
+        return classical(m, n, k)
+    p = algebra.partition(m, n, k, plan.dims)
+    t = 0.0
+    if p.ms > 0 and p.ns > 0 and p.ks > 0:
+        c = _core(model, plan, p)
+        if c["presum_s"] > 0:
+            t += c["presum_s"] + model.launch_s
+        if c["overlap"]:
+            t += max(launch(c["sm_s"], c["units"]), c["c_s"])
+        else:
+            t += launch(c["sm_s"], c["units"]) + c["c_s"]
+    for (mm, nn, kk) in _strips(p, m, n, k):
+        t += classical(mm, nn, kk)
+    return t
 
 
 def rank_candidates(model: B200Model, shape: Sequence[int],
