@@ -1593,6 +1593,8 @@ struct fmm_batch {
     int ms, ns, ks;                // sub-block sizes
     int a_r, a_c, b_r, b_c, c_r, c_c;  // operand offsets (row, column) inside the problem
     bool presum;
+    int kk;                        // k extent of the products: ks, or ks rounded up to the k step
+                                   // when every product reads a zero-padded slot (ks % 8 != 0)
     int nA, nB;                    // pre-summed operand slots
     size_t ws_off;                 // byte offset of S (then T) in the workspace
     long long ldT;
@@ -1676,12 +1678,17 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
   j.c_r = c_r;
   j.c_c = c_c;
   j.presum = plan->rank > 1 && use_presum(plan, ms, ns, ks);
+  j.kk = ks;
   if (j.presum) {
-    j.nA = (int)plan->plistA.size();
-    j.nB = (int)plan->plistB.size();
-    j.ldT = ks + (ks & 1);
+    // as in run_fmm: with ks not a multiple of the k step every product gets its own slot,
+    // zero-padded to whole k steps, so the phase keeps the direct variant
+    const bool padded = ks % fmm::BK != 0;
+    j.kk = padded ? (ks + fmm::BK - 1) / fmm::BK * fmm::BK : ks;
+    j.nA = padded ? plan->rank : (int)plan->plistA.size();
+    j.nB = padded ? plan->rank : (int)plan->plistB.size();
+    j.ldT = padded ? j.kk : ks + (ks & 1);
     j.ws_off = b->ws_bytes;
-    b->ws_bytes += sizeof(double) * ((size_t)ms * ks * j.nA + (size_t)j.ldT * ns * j.nB);
+    b->ws_bytes += sizeof(double) * ((size_t)ms * j.kk * j.nA + (size_t)j.ldT * ns * j.nB);
     b->ws_bytes = (b->ws_bytes + 255) & ~(size_t)255;
     b->max_slots = std::max(b->max_slots, std::max(j.nA, j.nB));
     b->max_lincomb_chunks = std::max({b->max_lincomb_chunks, lincomb_chunks((long long)(ms + 1) / 2 * ks),
@@ -1697,7 +1704,7 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
   j.cost = (double)plan->rank / j.chunks * ((ks + fmm::BK - 1) / fmm::BK);
   // direct staging: operands are single unit-coefficient blocks (pre-summed or classical)
   // and every k step stays inside them
-  if (!((j.presum || plan->rank == 1) && whole_k_steps(j.grid, ks))) b->direct[phase] = false;
+  if (!((j.presum || plan->rank == 1) && whole_k_steps(j.grid, j.kk))) b->direct[phase] = false;
   b->jobs[phase].push_back(j);
 }
 
@@ -1854,10 +1861,12 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
     const long long am = (long long)j.grid[0] * j.ms, ak = (long long)j.grid[1] * j.ks,
                     bn = (long long)j.grid[2] * j.ns;
     if (j.presum) {
+      const bool padded = j.kk != j.ks;
       const double* S = reinterpret_cast<const double*>(b->d_ws + j.ws_off);
-      const double* T = S + (size_t)j.ms * j.ks * j.nA;
-      a.prods = d.prods_ps;
-      a.terms = d.terms_ps;
+      const double* T = S + (size_t)j.ms * j.kk * j.nA;
+      a.ks = j.kk;
+      a.prods = padded ? d.prods_all : d.prods_ps;
+      a.terms = padded ? d.terms_all : d.terms_ps;
       a.Aw = S;
       a.ldaw = j.ms;
       a.Bw = T;
@@ -1877,10 +1886,10 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
         l.blk_col_stride = l.cols;
         l.out = const_cast<double*>(side == 0 ? S : T);
         l.ldo = side == 0 ? j.ms : j.ldT;
-        l.out_stride = l.ldo * l.cols;
+        l.out_stride = l.ldo * (side == 0 ? j.kk : l.cols);
         l.prods = d.prods;
         l.terms = d.terms;
-        l.plist = side == 0 ? d.plistA : d.plistB;
+        l.plist = padded ? d.plist_all : side == 0 ? d.plistA : d.plistB;
         l.side = side;
       }
     } else {
@@ -1895,12 +1904,12 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
               make_tensor_map(&a.tmB, a.B, ak, bn, lb, fmm::BK, fmm::BN) &&
               make_tensor_map(&a.tmB2, a.B, ak, bn, lb, fmm::TB_K, fmm::BN);
     if (ok && j.presum && j.nA > 0)
-      ok = make_tensor_map(&a.tmAw, a.Aw, j.ms, (long long)j.nA * j.ks, j.ms, fmm::BM, fmm::BK);
+      ok = make_tensor_map(&a.tmAw, a.Aw, j.ms, (long long)j.nA * j.kk, j.ms, fmm::BM, fmm::BK);
     else
       a.tmAw = a.tmA;
     if (ok && j.presum && j.nB > 0)
-      ok = make_tensor_map(&a.tmBw, a.Bw, j.ks, (long long)j.nB * j.ns, j.ldT, fmm::BK, fmm::BN) &&
-           make_tensor_map(&a.tmBw2, a.Bw, j.ks, (long long)j.nB * j.ns, j.ldT, fmm::TB_K, fmm::BN);
+      ok = make_tensor_map(&a.tmBw, a.Bw, j.kk, (long long)j.nB * j.ns, j.ldT, fmm::BK, fmm::BN) &&
+           make_tensor_map(&a.tmBw2, a.Bw, j.kk, (long long)j.nB * j.ns, j.ldT, fmm::TB_K, fmm::BN);
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
     tma = tma && ok;
@@ -1984,6 +1993,18 @@ int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool t
     g_launches.fetch_add(1, std::memory_order_relaxed);
     FMM_CUDA_TRY(cudaGetLastError());
   }
+  // zero padding of the padded slots (k columns [ks, kk) of every S slot, rows [ks, kk)
+  // of every T slot column): the sums fill only [0, ks)
+  for (int ph = 0; ph < 2; ++ph)
+    for (const auto& j : b->jobs[ph]) {
+      if (!j.presum || j.kk == j.ks) continue;
+      char* S = b->d_ws + j.ws_off;
+      char* T = S + sizeof(double) * (size_t)j.ms * j.kk * j.nA;
+      FMM_CUDA_TRY(cudaMemset2DAsync(S + sizeof(double) * (size_t)j.ms * j.ks, sizeof(double) * (size_t)j.ms * j.kk, 0,
+                                     sizeof(double) * (size_t)j.ms * (j.kk - j.ks), j.nA, st));
+      FMM_CUDA_TRY(cudaMemset2DAsync(T + sizeof(double) * j.ks, sizeof(double) * (size_t)j.kk, 0,
+                                     sizeof(double) * (j.kk - j.ks), (size_t)j.nB * j.ns, st));
+    }
   if (n_lc > 0) {
     ProfScope pf(K_LINCOMB_BATCH, st);
     fmm::fmm_lincomb_batch_kernel<<<dim3((unsigned)b->max_slots, b->max_lincomb_chunks, (unsigned)n_lc), 256, 0, st>>>(
