@@ -93,7 +93,10 @@ int fmm_plain_dgemm_dev(int m, int n, int k, const double *A, long lda, const do
                         long ldc, void *stream);
 
 /* Host-pointer FMM with an explicit plan: copies A, B, C to the device, runs, copies C
- * back, synchronises.  The drop-in symbols above call this with the default plan. */
+ * back, synchronises.  The drop-in symbols above call this with the default plan.  When C
+ * has at least 2^22 elements and n >= 4096 the call runs as up to four column panels
+ * C[:, J] += A * B[:, J] whose copies in and out overlap the compute (fastest with pinned
+ * host buffers); each panel is partitioned like an m x |J| x k call. */
 int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, const double *A, int lda,
                    const double *B, int ldb, double *C, int ldc);
 
