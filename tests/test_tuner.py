@@ -75,3 +75,47 @@ def test_sweep_families_match_the_reference_ranges():
         sweep.shapes("cube", [1])
     m = tuner.B200Model()
     assert sweep.model_gflops("222-1", 8192, 8192, 8192, m) > sweep.model_gflops("classical", 8192, 8192, 8192, m)
+
+
+def test_tile_work_counts_edge_fragments():
+    assert tuner._tile_work(256, 384) == 6.0  # whole tiles
+    # 40 rows past the last whole tile: 3 of 8 16-row fragments
+    assert tuner._tile_work(128 + 40, 128) == 1.0 + 3 / 8
+    # 40 columns past it: 2 of 4 32-column groups
+    assert tuner._tile_work(128, 128 + 40) == 1.0 + 2 / 4
+    # corner: the cheaper of the two edge forms
+    assert tuner._tile_work(40, 40) == min(3 / 8, 2 / 4)
+    assert tuner._tile_work(0, 128) == 0.0
+
+
+# Single-problem times (ms) measured on B200 with this library's current kernels; the model's
+# stated fit is 9 % RMS of the log ratio over these points.
+MEASURED_MS = {
+    ("222-1_333-1", 4000, 3840, 2000): 2.659, ("222-1_333-1", 4000, 8000, 2000): 5.264,
+    ("222-1_333-1", 4096, 4096, 4096): 5.077, ("222-1_333-1", 3000, 3000, 3000): 2.122,
+    ("222-1_333-1", 14400, 3840, 480): 3.807, ("222-1_333-1", 16384, 16384, 16384): 205.42,
+    ("222-1_333-1", 4000, 16000, 2000): 9.65, ("222-1_333-1", 14400, 14400, 480): 12.76,
+    ("222-1", 1024, 1024, 1024): 0.138, ("222-1", 2048, 2048, 2048): 0.64,
+    ("222-1", 6000, 6000, 6000): 11.79, ("222-1", 16384, 16384, 16384): 219.7,
+    ("222-2", 2048, 2048, 2048): 0.604, ("222-2", 3000, 3000, 3000): 1.874,
+    ("classical", 3000, 3000, 3000): 1.67, ("classical", 16384, 16384, 16384): 249.1,
+    ("classical", 2048, 2048, 2048): 0.577,
+}
+
+
+def test_single_problem_model_fits_the_measurements():
+    m = tuner.B200Model()
+    logs = [math.log(tuner.model_time_single(m, a, *s) * 1e3 / t) for (a, *s), t in MEASURED_MS.items()]
+    rms = math.sqrt(sum(x * x for x in logs) / len(logs))
+    assert rms < 0.10
+    assert max(abs(x) for x in logs) < 0.25
+
+
+def test_single_problem_view_adds_waves_and_launches():
+    m = tuner.B200Model()
+    # a small problem leaves SMs idle and pays launch latency: slower than its batch share
+    assert tuner.model_time_single(m, "222-1", 1024, 1024, 1024) > 1.5 * tuner.model_time(m, "222-1", 1024, 1024, 1024)
+    # a large one fills many waves: the two views agree closely
+    a = tuner.model_time_single(m, "222-1", 16384, 16384, 16384)
+    b = tuner.model_time(m, "222-1", 16384, 16384, 16384)
+    assert abs(a / b - 1) < 0.05
