@@ -15,9 +15,10 @@
 //   * multi-destination C update (meta/abc_micro_kernel_gen.py:147-244)
 //     -> epilogue C_l += W[l,r] * M_r for every nonzero W of product r.  A work unit
 //        owns one tile position in all C blocks for a range of products; when products
-//        are split over several units, per-tile tickets order the units' C updates
-//        (bounded spin, error flag on timeout), so no two CTAs ever update the same C
-//        element at once and products are applied in order r = 0..R-1.
+//        are split over several units, tickets per tile (or, in the direct variant with
+//        few tile positions, per tile and C block) order the units' C updates (bounded
+//        spin, error flag on timeout), so no two CTAs ever update the same C element at
+//        once and every element receives its products in order r = 0..R-1.
 //   * M_Add / S_Add / T_Add (meta/ab_gen_mix.py:341-372, meta/naive_gen_mix.py:60-137)
 //     -> fmm_lincomb_kernel / fmm_lincomb_batch_kernel (operand sums formed in HBM, also
 //        used by the ABC pack type for large sub-blocks), fmm_combine_kernel (every
@@ -143,7 +144,7 @@ struct GemmArgs {
   int tiles_m, tiles_n;
   int chunks;       // products are split into `chunks` consecutive ranges per tile
   int mode;
-  int* tickets;     // per tile: chunks completed (zeroed before launch); used when chunks > 1
+  int* tickets;     // per tile (nbt = 0): chunks completed; zeroed before launch; used when chunks > 1
   unsigned* status; // device status word (StatusBits)
   int nbt;          // > 0 (direct variant, one product per unit): tickets per (tile, C block),
   int nbc;          // nbt = C blocks, index tile * nbt + row * nbc + col, counting the block's
