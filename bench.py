@@ -35,7 +35,6 @@ SHAPES = [(16384, 16384, 16384), (14400, 14400, 480), (4000, 16000, 2000)]
 WORKLOAD = "222-1x333-1 abc FP64 C+=A*B over 16384^3, 14400x14400x480, 4000x16000x2000"
 METRIC = "effective TFLOPS (2mnk/t), 222-1x333-1 abc FP64"
 UNIT = "TFLOP/s"
-CPU_SAMPLE = (14400, 14400, 480)
 # DRAM traffic of the FMM products launches per executed core flop, from a one-pass ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of one timed step of this workload:
 # 226.9 GB over 6.88e12 executed flops (16384^3: 153.9 GB, 14400x14400x480: 55.7 GB,
@@ -117,52 +116,95 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
 
 
-def oracle_sample_tflops(shape, reps=1):
-    """CPU restatement of the reference's abc algorithm (the oracle) on the host cores."""
-    import numpy as np
+REF_PRODUCTS_PER_STEP = 8  # products of the 16384^3 call's FMM core timed per reference step
 
-    from fmm_gen_b200 import algebra, runtime
-    from oracle import cpu
 
-    plan = algebra.make_plan(ALGS, LEVELS)
-    dims, nterms, rows, cols, coefs = runtime.plan_tables(plan)
-    tables = (dims, plan.rank, nterms, rows, cols, coefs)
-    m, n, k = shape
-    rng = np.random.default_rng(99)
-    A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
-    B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
-    C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
-    times = []
-    for _ in range(reps):
+class OracleWorkload:
+    """The oracle -- the CPU restatement of the reference's generated abc code, OpenMP over
+    the host cores -- on this bench's workload, with every input made (seeded) and every
+    table built before anything is timed.
+
+    One step runs the 14400x14400x480 and 4000x16000x2000 calls whole, and samples the
+    16384^3 call: its FMM core (16368 x 16368 x 16380; the fringe strips are 0.2 % of its
+    flops) run over REF_PRODUCTS_PER_STEP of its 161 products, a different group each step
+    (all 161 after 21 steps), credited that share of the core's 2mnk.  A whole 16384^3 call
+    takes ~35 s on 16 cores; the sample keeps a step near 4 s.  step() returns the credited
+    effective flops and the seconds spent in the oracle calls alone."""
+
+    def __init__(self, seed: int = 99):
+        import numpy as np
+
+        from fmm_gen_b200 import algebra, runtime
+        from oracle import cpu
+
+        self.cpu = cpu
+        plan = algebra.make_plan(ALGS, LEVELS)
+        dims, nterms, rows, cols, coefs = runtime.plan_tables(plan)
+        self.tables = (dims, plan.rank, nterms, rows, cols, coefs)
+        self.R = plan.rank
+        rng = np.random.default_rng(seed)
+        self.mats = []
+        for (m, n, k) in SHAPES:
+            A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+            B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+            C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+            self.mats.append((A, B, C))
+        m, n, k = SHAPES[0]
+        self.core = algebra.partition(m, n, k, plan.dims)
+        P = REF_PRODUCTS_PER_STEP
+        ngroups = (self.R + P - 1) // P
+        self.groups = [[(g * P + i) % self.R for i in range(P)] for g in range(ngroups)]
+        self.subsets = [cpu.product_subset(self.tables, grp) for grp in self.groups]
+        self.step_no = 0
+        self.cores = cpu.num_threads()
+
+    def step(self):
+        cpu, pc = self.cpu, self.core
+        secs, flops = 0.0, 0.0
+        for (m, n, k), (A, B, C) in zip(SHAPES[1:], self.mats[1:]):
+            t0 = time.perf_counter()
+            cpu.fmm(self.tables, PACK, A, B, C)
+            secs += time.perf_counter() - t0
+            flops += 2.0 * m * n * k
+        A, B, C = self.mats[0]
+        sub = self.subsets[self.step_no % len(self.subsets)]
+        Ac, Bc, Cc = A[:pc.md, :pc.kd], B[:pc.kd, :pc.nd], C[:pc.md, :pc.nd]
         t0 = time.perf_counter()
-        cpu.fmm(tables, PACK, A, B, C)
-        times.append(time.perf_counter() - t0)
-    return 2.0 * m * n * k / min(times) / 1e12, cpu.num_threads(), times
+        cpu.fmm(sub, PACK, Ac, Bc, Cc)
+        secs += time.perf_counter() - t0
+        flops += 2.0 * pc.md * pc.nd * pc.kd * REF_PRODUCTS_PER_STEP / self.R
+        self.step_no += 1
+        return flops, secs
+
+    def describe(self, steps):
+        return (f"oracle/fmm_oracle.c (the reference's abc arithmetic) on {self.cores} host threads; per step "
+                f"14400x14400x480 and 4000x16000x2000 whole plus {REF_PRODUCTS_PER_STEP} of the 161 products of "
+                f"the 16384^3 call's FMM core (16368x16368x16380), rotating, credited {REF_PRODUCTS_PER_STEP}/161 "
+                f"of its 2mnk; {steps} steps; inputs generated before timing")
 
 
 def run_reference(args, rank):
     """--impl reference: the CPU restatement of the reference's algorithm, timed on the host."""
     if rank != 0:
         return
-    sample = CPU_SAMPLE
+    wl = OracleWorkload()
     for _ in range(args.warmup):
-        oracle_sample_tflops(sample)
-    t0 = time.perf_counter()
-    per = []
+        wl.step()
+    flops, secs = 0.0, 0.0
     for _ in range(args.steps):
-        v, cores, ts = oracle_sample_tflops(sample)
-        per.append(ts[0])
-    total = time.perf_counter() - t0
-    m, n, k = sample
-    value = 2.0 * m * n * k * args.steps / total / 1e12
+        f, t = wl.step()
+        flops += f
+        secs += t
+    value = flops / secs / 1e12
+    sample = wl.describe(args.steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_shape": list(sample), "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"one 222-1x333-1 abc C+=A*B at {m}x{n}x{k} (the workload's rank-k shape) "
-                                   "per step, oracle/fmm_oracle.c with OpenMP"},
+        "config": {"workload": WORKLOAD, "algorithm": "222-1_333-1", "pack_type": PACK,
+                   "shapes": [list(s) for s in SHAPES], "inputs": "A,B,C ~ U(-1,1), seeded",
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": wl.cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -309,17 +351,18 @@ def batch_512(rt, torch, dev, steps=3):
     torch.cuda.current_stream(dev).wait_stream(s)
     torch.cuda.synchronize()
     graph = torch.cuda.CUDAGraph()
+    n0 = rt.kernel_launch_count()
     with torch.cuda.graph(graph):
         batch.run(As, Bs, Cs)
+    launches_per_replay = rt.kernel_launch_count() - n0  # kernels the library put into the graph
     graph.replay()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with rt.KernelTimer() as kt:
-        e0.record()
-        for _ in range(steps):
-            graph.replay()
-        e1.record()
-        torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     del graph
     batch.close()
@@ -327,7 +370,7 @@ def batch_512(rt, torch, dev, steps=3):
            "ms": ms, "tflops_effective": flops / (ms * 1e-3) / 1e12,
            "all_classical_ms": classical_ms, "model_ms": model_ms,
            "choices": rep.counts(), "tune_s": tune_s, "tune_trials": rep.trials,
-           "launches_per_replay": {k: v / steps for k, v in kt.count.items() if v}}
+           "launches_per_replay": launches_per_replay}
     del As, Bs, Cs
     torch.cuda.empty_cache()
     return out
@@ -436,9 +479,11 @@ def main():
     clk = clocks.summary()
 
     # ---- dominant kernel roofline (FP64 DMMA bound) ----
-    core_name = "fmm_gemm_kernel[fmm products]"
-    core_ms = kt.ms[core_name]
-    core_launches = kt.count[core_name]
+    # the FMM products launches: the direct variant (pre-summed operands) or the folding kernel
+    kinds = [k for k in ("fmm_gemm_direct_kernel[fmm products]", "fmm_gemm_kernel[fmm products]") if kt.count.get(k)]
+    core_name = max(kinds, key=lambda k: kt.ms[k]) if kinds else "fmm_gemm_direct_kernel[fmm products]"
+    core_ms = sum(kt.ms[k] for k in kinds)
+    core_launches = sum(kt.count[k] for k in kinds)
     cflops = core_flops(plan.algebra, SHAPES) * args.steps
     achieved = cflops / (core_ms * 1e-3) / 1e12 if core_ms > 0 else None
 
@@ -530,10 +575,16 @@ def main():
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, ts = oracle_sample_tflops(CPU_SAMPLE)
-        cpu_baseline = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                        "sample": f"one 222-1x333-1 abc C+=A*B at {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} "
-                                  f"(the workload's rank-k shape), oracle/fmm_oracle.c with OpenMP, {ts[0]:.1f} s"}
+        wl = OracleWorkload()
+        wl.step()  # warm-up
+        cf, cs = 0.0, 0.0
+        for _ in range(3):
+            f, t = wl.step()
+            cf += f
+            cs += t
+        cpu_baseline = {"value": cf / cs / 1e12, "unit": UNIT, "cores": wl.cores, "kind": "port",
+                        "sample": wl.describe(3) + f", {cs:.1f} s"}
+        del wl
 
     if rank == 0:
         per_launch_flops = cflops / max(core_launches, 1)

@@ -28,11 +28,14 @@
 namespace {
 
 constexpr int kMaxDevices = 64;
+constexpr int kBatchCounters = 2;  // a batch's per-phase work-unit counters, ahead of its tickets
 constexpr int kMR = 8;  // register-tile granularity of the FMM/fringe split (bl_config.h:16-17)
 constexpr int kNR = 4;
 
 std::atomic<long long> g_launches{0};
 thread_local int t_last_error = FMM_OK;
+// Byte written into every ticket before a launch (fmm_debug_set): 0 in normal operation.
+int g_ticket_fill = 0;
 
 // Optional per-kernel timing: when enabled, every launch is bracketed by CUDA events on
 // its own stream; fmm_profile_end() sums the durations per kernel kind.
@@ -47,13 +50,17 @@ enum KernelKind {
   K_LINCOMB_BATCH = 7,
   K_PITCH_COPY = 8,
   K_COMBINE = 9,
-  K_NUM = 10
+  K_GEMM_FMM_DIRECT = 10,        // the same launches when they run the direct variant
+  K_GEMM_CLASSICAL_DIRECT = 11,
+  K_NUM = 12
 };
 const char* const kKernelNames[K_NUM] = {"fmm_gemm_kernel[fmm products]", "fmm_gemm_kernel[classical]",
                                          "fmm_lincomb_kernel", "fmm_scatter_kernel",
                                          "fmm_split_operands_kernel", "fmm_split_gemm_kernel",
                                          "fmm_gemm_batch_kernel", "fmm_lincomb_batch_kernel",
-                                         "fmm_pitch_copy_kernel", "fmm_combine_kernel"};
+                                         "fmm_pitch_copy_kernel", "fmm_combine_kernel",
+                                         "fmm_gemm_direct_kernel[fmm products]",
+                                         "fmm_gemm_direct_kernel[classical]"};
 struct ProfRec {
   int kind;
   cudaEvent_t e0, e1;
@@ -99,6 +106,15 @@ struct DevTables {
   bool ready = false;
 };
 
+// Tables of a k split (see ksplit_tables): base tables (one of the TableBase forms) with
+// every product r split into S products (r, p) over k range p of its operands.
+enum TableBase : int { BASE_ORIG = 0, BASE_PS = 1, BASE_ALL = 2 };
+struct KSplitTables {
+  int base = 0, S = 0, dev = -1;
+  fmm::Prod* prods = nullptr;
+  fmm::Term* terms = nullptr;
+};
+
 }  // namespace
 
 struct fmm_plan {
@@ -123,6 +139,7 @@ struct fmm_plan {
   std::vector<fmm::Term> terms_all;
   std::mutex mu;
   DevTables dev[kMaxDevices];
+  std::vector<KSplitTables> ksplit;  // uploaded k-split tables (any device), built on first use
 };
 
 namespace {
@@ -195,6 +212,80 @@ int device_tables(const fmm_plan* cp, DevTables** out) {
     if (rc != FMM_OK) return rc;
   }
   *out = &d;
+  return FMM_OK;
+}
+
+// k split of a plan's products: product r (k extent ks) becomes S products (r, p), p = 0..S-1,
+// each over k range [p ks/S, (p+1) ks/S) of r's operands, with r's C terms.  A work unit then
+// covers a product's k range part, so a launch with too few units for whole waves of the
+// SMs gets S times as many, shorter ones.  The C update is linear in the product, so the
+// parts' updates, applied in order (r, 0), (r, 1), ... under the same tickets, sum to r's.
+// With the part depth ks' = ks / S every operand term keeps its block and indexes part p by
+// its k block coordinate: an A term (row, col) becomes (row, col S + p) (A column offset
+// col ks + p ks' = (col S + p) ks'), a B term (row, col) becomes (row S + p, col); this holds
+// for blocks of A and B and for the slots of the pre-summed workspaces alike.  C terms keep
+// their block; their per-block ticket position (pad) counts the split products.
+void ksplit_build(const fmm_plan* p, int base, int S, std::vector<fmm::Prod>* op, std::vector<fmm::Term>* ot) {
+  const std::vector<fmm::Prod>& prods = base == BASE_PS ? p->prods_ps : base == BASE_ALL ? p->prods_all : p->prods;
+  const std::vector<fmm::Term>& terms = base == BASE_PS ? p->terms_ps : base == BASE_ALL ? p->terms_all : p->terms;
+  std::vector<int> cnt((size_t)p->dims[0] * p->dims[2], 0);
+  for (const fmm::Prod& pr : prods) {
+    for (int q = 0; q < S; ++q) {
+      fmm::Prod v = pr;
+      v.a0 = (int)ot->size();
+      for (int t = 0; t < pr.na; ++t) {
+        fmm::Term x = terms[pr.a0 + t];
+        x.col = x.col * S + q;
+        ot->push_back(x);
+      }
+      v.b0 = (int)ot->size();
+      for (int t = 0; t < pr.nb; ++t) {
+        fmm::Term x = terms[pr.b0 + t];
+        x.row = x.row * S + q;
+        ot->push_back(x);
+      }
+      v.c0 = (int)ot->size();
+      for (int t = 0; t < pr.nc; ++t) {
+        fmm::Term x = terms[pr.c0 + t];
+        x.pad = cnt[(size_t)x.row * p->dims[2] + x.col]++;
+        ot->push_back(x);
+      }
+      op->push_back(v);
+    }
+  }
+}
+
+// The k-split tables of a plan on the current device (uploaded on first use).
+int ksplit_tables(const fmm_plan* cp, int base, int S, const fmm::Prod** prods, const fmm::Term** terms) {
+  fmm_plan* p = const_cast<fmm_plan*>(cp);
+  int dev = 0;
+  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(p->mu);
+  for (const auto& t : p->ksplit)
+    if (t.base == base && t.S == S && t.dev == dev) {
+      *prods = t.prods;
+      *terms = t.terms;
+      return FMM_OK;
+    }
+  std::vector<fmm::Prod> vp;
+  std::vector<fmm::Term> vt;
+  ksplit_build(p, base, S, &vp, &vt);
+  KSplitTables t;
+  t.base = base;
+  t.S = S;
+  t.dev = dev;
+  FMM_CUDA_TRY(cudaMalloc(&t.prods, sizeof(fmm::Prod) * vp.size()));
+  cudaError_t e = cudaMalloc(&t.terms, sizeof(fmm::Term) * vt.size());
+  if (e == cudaSuccess) e = cudaMemcpy(t.prods, vp.data(), sizeof(fmm::Prod) * vp.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t.terms, vt.data(), sizeof(fmm::Term) * vt.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(t.prods);
+    if (t.terms) cudaFree(t.terms);
+    return cuda_status(e);
+  }
+  p->ksplit.push_back(t);
+  *prods = t.prods;
+  *terms = t.terms;
   return FMM_OK;
 }
 
@@ -390,6 +481,32 @@ int choose_chunks(int ntiles, int nprod, int nsm) {
   return nprod;
 }
 
+// k split (ksplit_build) for a launch of `units` work units of ks deep products on nsm SMs.
+// A launch of few units spends its last wave partly idle: 222-1 at 2048^3 has 448 units
+// on 148 SMs, 3.03 waves whose last holds 4 units.  Splitting every product's k range into S
+// parts gives S times the units, each S times shorter; the modelled time
+// ceil(units S / nsm) (ks / (8 S) + kUnitOverheadSteps) k steps picks S in 1..8 (parts of
+// whole k steps, at least kMinPartSteps deep; a split must gain 3 %).  Launches of many waves
+// keep S = 1.
+constexpr int kUnitOverheadSteps = 4;  // per-unit cost beyond its k steps (hand-off, C tile traffic)
+constexpr int kMinPartSteps = 16;
+int choose_ksplit(long long units, int ks, int nsm) {
+  if (units <= 0 || nsm <= 0 || units >= 8LL * nsm || ks % fmm::BK != 0) return 1;
+  const long long nks = ks / fmm::BK;
+  auto cost = [&](int S) { return ((units * S + nsm - 1) / nsm) * (double)(nks / S + kUnitOverheadSteps); };
+  int best = 1;
+  double best_cost = cost(1);
+  for (int S = 2; S <= 8; ++S) {
+    if (nks % S != 0 || nks / S < kMinPartSteps) continue;
+    const double c = cost(S);
+    if (c < 0.97 * best_cost) {
+      best = S;
+      best_cost = c;
+    }
+  }
+  return best;
+}
+
 // Launch the persistent DMMA GEMM over sub-blocks of size ms x ks x ns.
 // Workspaces of pre-summed operands (slot j of S: ms x ks, of T: ks x ns, block columns).
 struct PresumOps {
@@ -414,11 +531,14 @@ bool whole_k_steps(const int grid_dims[3], int ks) {
 // direct_ok: every product's operands are single unit-coefficient blocks (pre-summed
 // products, the classical plan), so with TMA staging and whole k steps the direct variant
 // (epilogue on the otherwise idle folding warps, overlapping the next product) can run.
+// ksplit > 1: prods / terms are k-split tables (ksplit_tables) with nprod = R * ksplit products
+// of depth ks / ksplit, a whole number of k steps; ks is the operands' full depth.
 int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
                 int mode, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
                 double* C, long long ldc, double* M, long long ldm, long long m_stride, int ms, int ns, int ks,
-                cudaStream_t st, bool direct_ok = false, int ks_orig = -1) {
+                cudaStream_t st, bool direct_ok = false, int ks_orig = -1, int ksplit = 1) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
+  if (ksplit < 1 || ks % ksplit != 0 || (ksplit > 1 && (ks / ksplit) % fmm::BK != 0)) return FMM_E_INVALID;
   int dev = 0;
   int rc = configure_kernel(&dev);
   if (rc != FMM_OK) return rc;
@@ -434,7 +554,7 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
   a.m_stride = m_stride;
   a.ms = ms;
   a.ns = ns;
-  a.ks = ks;
+  a.ks = ks / ksplit;
   a.prods = prods;
   a.terms = terms;
   a.Aw = ps.S ? ps.S : A;
@@ -472,7 +592,7 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
   }
-  const bool direct = direct_ok && tma && whole_k_steps(grid_dims, ks);
+  const bool direct = direct_ok && tma && whole_k_steps(grid_dims, a.ks);
   // Per-tile tickets keep a tile's C updates in product order.  With few tile positions
   // (at most half as many as SMs) the units of one position run at the same time and their
   // epilogues form one chain of all R products; there the direct variant (one product per
@@ -483,19 +603,25 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
   // -> 5.08 ms; 222-2 2048^3 0.88 -> 0.60 ms; 222-1 1024^3 0.17 -> 0.14 ms.  With more
   // positions the extra barrier per C term costs more than it frees (14400^2 x 480, 361
   // positions: 12.5 -> 14.0 ms; 4000 x 16000 x 2000, 126 positions: 9.5 -> 9.9 ms).
-  int* tickets = nullptr;
+  // [0]: the launch's work-unit counter; then the tickets
+  size_t nt = 0;
   if (mode == fmm::MODE_ACCUM_C && a.chunks > 1) {
     if (direct && a.chunks == nprod && 2 * ntiles <= sm_count[dev]) {
       a.nbt = grid_dims[0] * grid_dims[2];
       a.nbc = grid_dims[2];
     }
-    const size_t nt = (size_t)ntiles * (a.nbt > 0 ? a.nbt : 1);
-    FMM_CUDA_TRY(cudaMallocAsync((void**)&tickets, sizeof(int) * nt, st));
-    FMM_CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int) * nt, st));
+    nt = (size_t)ntiles * (a.nbt > 0 ? a.nbt : 1);
   }
-  a.tickets = tickets;
+  int* tickets = nullptr;
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&tickets, sizeof(int) * (nt + 1), st));
+  FMM_CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int) * (nt + 1), st));
+  if (nt > 0 && g_ticket_fill != 0)
+    FMM_CUDA_TRY(cudaMemsetAsync(tickets + 1, g_ticket_fill, sizeof(int) * nt, st));
+  a.counter = tickets;
+  a.tickets = nt > 0 ? tickets + 1 : nullptr;
   {
-    ProfScope ps(kind, st);
+    const int pkind = !direct ? kind : (kind == K_GEMM_FMM ? K_GEMM_FMM_DIRECT : K_GEMM_CLASSICAL_DIRECT);
+    ProfScope ps(pkind, st);
     if (direct)
       fmm::fmm_gemm_direct_kernel<<<grid, fmm::NTHREADS, fmm::SMEM_BYTES_DIRECT, st>>>(a);
     else if (tma)
@@ -514,12 +640,31 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
 
 const int kUnitGrid[3] = {1, 1, 1};
 
+int sm_count_current() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+  return sm_count[dev];
+}
+
 int plain_gemm(int m, int n, int k, const double* A, long long lda, const double* B, long long ldb, double* C,
                long long ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0 || k <= 0) return FMM_OK;
   DevTables* d = nullptr;
   int rc = device_tables(classical_plan(), &d);
   if (rc != FMM_OK) return rc;
+  int dev = 0;
+  rc = configure_kernel(&dev);
+  if (rc != FMM_OK) return rc;
+  const long long tiles = (long long)((m + fmm::BM - 1) / fmm::BM) * ((n + fmm::BN - 1) / fmm::BN);
+  const int S = choose_ksplit(tiles, k, sm_count[dev]);
+  if (S > 1) {
+    const fmm::Prod* vp = nullptr;
+    const fmm::Term* vt = nullptr;
+    rc = ksplit_tables(classical_plan(), BASE_ORIG, S, &vp, &vt);
+    if (rc != FMM_OK) return rc;
+    return launch_gemm(K_GEMM_CLASSICAL, vp, vt, kUnitGrid, S, fmm::MODE_ACCUM_C, A, lda, B, ldb, PresumOps{}, C,
+                       ldc, nullptr, 0, 0, m, n, k, st, true, -1, S);
+  }
   return launch_gemm(K_GEMM_CLASSICAL, d->prods, d->terms, kUnitGrid, 1, fmm::MODE_ACCUM_C, A, lda, B, ldb,
                      PresumOps{}, C, ldc, nullptr, 0, 0, m, n, k, st, true);
 }
@@ -615,6 +760,26 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
 bool use_presum(const fmm_plan* plan, int ms, int ns, int ks) {
   if (plan->plistA.empty() && plan->plistB.empty()) return false;
   return (long long)ms * ns >= (1LL << 17) && ks >= 64;
+}
+
+// ABC schedule for pre-summed products: the multi-destination epilogue (C_l += W[l,r] M_r
+// straight from each product tile) or, when that C traffic dominates, the products stored
+// to a workspace and one combine pass (every M_r and C element crossing HBM once).  The
+// epilogue moves 16 nnz(W) ms ns bytes of C while the DMMAs run; the stored schedule writes
+// 8 R ms ns bytes of product tiles (also during the DMMAs), then the combine pass moves
+// 8 (R + 2 blocks) ms ns bytes.  Rates measured on B200: DMMA products 33 TFLOP/s executed,
+// the epilogue's C traffic 4.6 TB/s (222-1 x 333-1 at 14400 x 14400 x 480: 55.7 GB in
+// 12.2 ms), product stores 6 TB/s, the combine pass 3.3 TB/s.  The stored schedule must
+// gain 10 %.  It is the reference's own trade between its ABC and AB variants
+// (meta/model_gen.py:87-95 counts the C memory operations of each).
+bool prefer_stored_products(const fmm_plan* plan, int ms, int ns, int ks) {
+  const double mn = (double)ms * ns;
+  const int nblk = plan->dims[0] * plan->dims[2];
+  const double t_mma = 2.0 * plan->rank * mn * ks / 33e12;
+  const double t_epi = 16.0 * plan->n_cterms * mn / 4.6e12;
+  const double t_store = 8.0 * plan->rank * mn / 6.0e12;
+  const double t_comb = 8.0 * (plan->rank + 2.0 * nblk) * mn / 3.3e12;
+  return std::max(t_mma, t_store) + t_comb < 0.9 * std::max(t_mma, t_epi);
 }
 
 int presum(const DevTables& d, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
@@ -748,14 +913,38 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
       const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
-      if (use_presum(plan, ms, ns, ks)) {
+      if (use_presum(plan, ms, ns, ks) && combine_fits(plan) && prefer_stored_products(plan, ms, ns, ks)) {
+        // C-traffic-bound shapes (small k per product): operand sums in HBM, each product
+        // stored by the direct variant, W applied by one combine pass
+        const long long mstride = (long long)ms * ns;
+        char* mws = nullptr;
+        FMM_CUDA_TRY(cudaMallocAsync((void**)&mws, sizeof(double) * (size_t)mstride * R, st));
+        double* M = reinterpret_cast<double*>(mws);
+        PresumPlan pp;
+        rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
+        if (rc == FMM_OK)
+          rc = launch_gemm(K_GEMM_FMM, pp.prods, pp.terms, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb, pp.ps,
+                           C, ldc, M, ms, mstride, ms, ns, pp.kk, st, true, ks);
+        if (rc == FMM_OK) rc = launch_combine(plan, *d, C, ldc, ms, ns, M, ms, mstride, st);
+        if (pp.ws) {
+          cudaError_t fe = cudaFreeAsync(pp.ws, st);
+          if (rc == FMM_OK) rc = cuda_status(fe);
+        }
+        cudaError_t fe = cudaFreeAsync(mws, st);
+        if (rc == FMM_OK) rc = cuda_status(fe);
+      } else if (use_presum(plan, ms, ns, ks)) {
         // U/V sums formed once per product in HBM (bandwidth-bound), then every
         // product reads single operands; products scattered into C in the epilogue.
         PresumPlan pp;
         rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
+        const long long units = (long long)((ms + fmm::BM - 1) / fmm::BM) * ((ns + fmm::BN - 1) / fmm::BN) * R;
+        const int S = choose_ksplit(units, pp.kk, sm_count_current());
+        const fmm::Prod* vp = pp.prods;
+        const fmm::Term* vt = pp.terms;
+        if (rc == FMM_OK && S > 1) rc = ksplit_tables(plan, pp.kk != ks ? BASE_ALL : BASE_PS, S, &vp, &vt);
         if (rc == FMM_OK)
-          rc = launch_gemm(K_GEMM_FMM, pp.prods, pp.terms, plan->dims, R, fmm::MODE_ACCUM_C, A, lda, B, ldb, pp.ps,
-                           C, ldc, nullptr, 0, 0, ms, ns, pp.kk, st, true, ks);
+          rc = launch_gemm(K_GEMM_FMM, vp, vt, plan->dims, R * S, fmm::MODE_ACCUM_C, A, lda, B, ldb, pp.ps, C, ldc,
+                           nullptr, 0, 0, ms, ns, pp.kk, st, true, ks, S);
         if (pp.ws) {
           cudaError_t fe = cudaFreeAsync(pp.ws, st);
           if (rc == FMM_OK) rc = cuda_status(fe);
@@ -873,15 +1062,20 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   return peel(m, n, k, A, lda, B, ldb, C, ldc, pm, pk, pn, st);
 }
 
+int noalloc_status(int dev, bool clear);  // the no-allocation entry point's status word (below)
+
 int device_status(bool clear) {
   int dev = 0;
   FMM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return FMM_E_UNSUPPORTED;
-  if (!smem_configured[dev]) return FMM_OK;
   unsigned v = 0;
-  FMM_CUDA_TRY(cudaMemcpy(&v, dev_status[dev], sizeof(unsigned), cudaMemcpyDeviceToHost));
-  if (clear && v) FMM_CUDA_TRY(cudaMemset(dev_status[dev], 0, sizeof(unsigned)));
-  return v ? FMM_E_TIMEOUT : FMM_OK;
+  if (smem_configured[dev]) {
+    FMM_CUDA_TRY(cudaMemcpy(&v, dev_status[dev], sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (clear && v) FMM_CUDA_TRY(cudaMemset(dev_status[dev], 0, sizeof(unsigned)));
+  }
+  const int rn = noalloc_status(dev, clear);
+  if (rn != FMM_OK && rn != FMM_E_TIMEOUT) return rn;
+  return (v || rn == FMM_E_TIMEOUT) ? FMM_E_TIMEOUT : FMM_OK;
 }
 
 // Host-pointer execution: stage A, B, C into device memory, run, copy C back.
@@ -1062,6 +1256,10 @@ int fmm_plan_destroy(fmm_plan* plan) {
     cudaFree(d.terms_all);
     cudaFree(d.plist_all);
   }
+  for (auto& t : plan->ksplit) {
+    cudaFree(t.prods);
+    cudaFree(t.terms);
+  }
   delete plan;
   return FMM_OK;
 }
@@ -1184,6 +1382,22 @@ long long fmm_kernel_launch_count(void) { return g_launches.load(); }
 
 int fmm_device_status(int clear) { return device_status(clear != 0); }
 
+int fmm_debug_set(int what, long long value) {
+  switch (what) {
+    case FMM_DEBUG_WAIT_LIMIT_NS: {
+      const unsigned long long v = value > 0 ? (unsigned long long)value : fmm::WAIT_LIMIT_NS;
+      FMM_CUDA_TRY(cudaMemcpyToSymbol(fmm::g_wait_limit_ns, &v, sizeof(v)));
+      return FMM_OK;
+    }
+    case FMM_DEBUG_TICKET_FILL:
+      if (value < 0 || value > 255) return FMM_E_INVALID;
+      g_ticket_fill = (int)value;
+      return FMM_OK;
+    default:
+      return FMM_E_INVALID;
+  }
+}
+
 int fmm_profile_begin(void) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   for (auto& r : g_prof) {
@@ -1235,7 +1449,7 @@ const char* fmm_profile_kind_name(int kind) { return (kind >= 0 && kind < K_NUM)
 // and code on latency-critical paths where an allocation (or the synchronisation a
 // cudaFree implies) is not acceptable.  fmm_dgemm_dev_noalloc() serves them: it runs the
 // ABC FMM with the operand sums folded during staging (no pre-summed workspace), and
-// keeps the only scratch the kernel needs -- per-tile tickets, the device status word --
+// keeps the only scratch the kernel needs -- per-tile tickets, a work-unit counter, the status word --
 // and the plan tables in one statically allocated device array.
 // ------------------------------------------------------------------------------------
 namespace {
@@ -1245,6 +1459,7 @@ constexpr int kNoAllocMaxProds = 1024;    // products of a plan
 constexpr int kNoAllocMaxTerms = 12288;   // A, B and C terms of a plan
 constexpr size_t kNoAllocTicketsOff = 0;
 constexpr size_t kNoAllocStatusOff = kNoAllocTicketsOff + sizeof(int) * kNoAllocMaxTiles;
+constexpr size_t kNoAllocCounterOff = kNoAllocStatusOff + 128;  // a launch's work-unit counter
 constexpr size_t kNoAllocProdsOff = kNoAllocStatusOff + 256;
 constexpr size_t kNoAllocTermsOff = kNoAllocProdsOff + sizeof(fmm::Prod) * (kNoAllocMaxProds + 1);
 constexpr size_t kNoAllocBytes = kNoAllocTermsOff + sizeof(fmm::Term) * (kNoAllocMaxTerms + 3);
@@ -1286,16 +1501,40 @@ int noalloc_setup(int dev) {
         g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
   }
-  g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  // The classical product used by the fringe strips never changes: its tables (product
+  // index kNoAllocMaxProds, terms after the plan's) are written here once, and the status
+  // word starts at zero.  Both copies are blocking, from memory that outlives them.
+  static const fmm::Prod classic{kNoAllocMaxTerms, 1, kNoAllocMaxTerms + 1, 1, kNoAllocMaxTerms + 2, 1};
+  static const fmm::Term classic_terms[3] = {{0, 0, 1.0, 0, 0}, {0, 0, 1.0, 0, 0}, {0, 0, 1.0, 0, 0}};
+  unsigned char* base = static_cast<unsigned char*>(p);
+  FMM_CUDA_TRY(cudaMemcpy(base + kNoAllocProdsOff + sizeof(fmm::Prod) * kNoAllocMaxProds, &classic, sizeof(classic),
+                          cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemcpy(base + kNoAllocTermsOff + sizeof(fmm::Term) * kNoAllocMaxTerms, classic_terms,
+                          sizeof(classic_terms), cudaMemcpyHostToDevice));
+  FMM_CUDA_TRY(cudaMemset(base + kNoAllocStatusOff, 0, sizeof(unsigned)));
+  g_noalloc_ptr[dev] = base;
   g_noalloc_ready[dev] = true;
   return FMM_OK;
+}
+
+int noalloc_status(int dev, bool clear) {
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ready[dev]) return FMM_OK;
+    base = g_noalloc_ptr[dev];
+  }
+  unsigned v = 0;
+  FMM_CUDA_TRY(cudaMemcpy(&v, base + kNoAllocStatusOff, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (clear && v) FMM_CUDA_TRY(cudaMemset(base + kNoAllocStatusOff, 0, sizeof(unsigned)));
+  return v ? FMM_E_TIMEOUT : FMM_OK;
 }
 
 // One launch of fmm_gemm_kernel in MODE_ACCUM_C with caller-provided tables, tickets and
 // status word (nothing allocated).
 int noalloc_launch(const fmm::Prod* prods, const fmm::Term* terms, const int grid_dims[3], int nprod,
                    const double* A, long long lda, const double* B, long long ldb, double* C, long long ldc,
-                   int ms, int ns, int ks, int* tickets, unsigned* status, int nsm, cudaStream_t st) {
+                   int ms, int ns, int ks, int* tickets, unsigned* status, int* counter, int nsm, cudaStream_t st) {
   if (ms <= 0 || ns <= 0 || ks <= 0 || nprod <= 0) return FMM_OK;
   fmm::GemmArgs a{};
   a.A = A;
@@ -1321,7 +1560,10 @@ int noalloc_launch(const fmm::Prod* prods, const fmm::Term* terms, const int gri
   const int ntiles = a.tiles_m * a.tiles_n;
   a.chunks = choose_chunks(ntiles, nprod, nsm);
   a.tickets = tickets;
+  if (a.chunks > 1 && ntiles > kNoAllocMaxTiles) return FMM_E_TOO_LARGE;  // tickets of one launch must fit
   if (a.chunks > 1) FMM_CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int) * ntiles, st));
+  a.counter = counter;
+  FMM_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), st));
   const long long units = (long long)ntiles * a.chunks;
   const unsigned grid = (unsigned)(units < nsm ? units : nsm);
   const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * ks,
@@ -1365,40 +1607,41 @@ extern "C" int fmm_dgemm_dev_noalloc(const fmm_plan* plan, int m, int n, int k, 
   unsigned char* base = g_noalloc_ptr[dev];
   int* tickets = reinterpret_cast<int*>(base + kNoAllocTicketsOff);
   unsigned* status = reinterpret_cast<unsigned*>(base + kNoAllocStatusOff);
+  int* counter = reinterpret_cast<int*>(base + kNoAllocCounterOff);
   fmm::Prod* prods = reinterpret_cast<fmm::Prod*>(base + kNoAllocProdsOff);
   fmm::Term* terms = reinterpret_cast<fmm::Term*>(base + kNoAllocTermsOff);
-  // plan tables, then the classical product (index kNoAllocMaxProds, terms after the plan's)
-  const fmm::Prod classic{kNoAllocMaxTerms, 1, kNoAllocMaxTerms + 1, 1, kNoAllocMaxTerms + 2, 1};
-  const fmm::Term one{0, 0, 1.0, 0, 0};
-  const fmm::Term classic_terms[3] = {one, one, one};
+  // the plan's tables (from the plan's own storage, which outlives the copy); the classical
+  // product of the fringe strips was written at set-up
   FMM_CUDA_TRY(cudaMemcpyAsync(prods, plan->prods.data(), sizeof(fmm::Prod) * plan->prods.size(),
                                cudaMemcpyHostToDevice, st));
   FMM_CUDA_TRY(cudaMemcpyAsync(terms, plan->terms.data(), sizeof(fmm::Term) * plan->terms.size(),
                                cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyAsync(prods + kNoAllocMaxProds, &classic, sizeof(classic), cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemcpyAsync(terms + kNoAllocMaxTerms, classic_terms, sizeof(classic_terms),
-                               cudaMemcpyHostToDevice, st));
-  FMM_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
   const int nsm = sm_count[dev] > 0 ? sm_count[dev] : 148;
-  rc = noalloc_launch(prods, terms, plan->dims, plan->rank, A, lda, B, ldb, C, ldc, ms, ns, ks, tickets, status, nsm,
-                      st);
+  rc = noalloc_launch(prods, terms, plan->dims, plan->rank, A, lda, B, ldb, C, ldc, ms, ns, ks, tickets, status,
+                      counter, nsm, st);
   // fringe GEMMs (same regions and order as the reference's dynamic peeling)
   const int mr = m - md, kr = k - kd, nr = n - nd;
   const fmm::Prod* cp = prods + kNoAllocMaxProds;
   if (rc == FMM_OK && kr > 0 && md > 0 && nd > 0)
     rc = noalloc_launch(cp, terms, kUnitGrid, 1, A + (long long)kd * lda, lda, B + kd, ldb, C, ldc, md, nd, kr,
-                        tickets, status, nsm, st);
+                        tickets, status, counter, nsm, st);
   if (rc == FMM_OK && nr > 0)
     rc = noalloc_launch(cp, terms, kUnitGrid, 1, A, lda, B + (long long)nd * ldb, ldb, C + (long long)nd * ldc, ldc, m,
-                        nr, k, tickets, status, nsm, st);
+                        nr, k, tickets, status, counter, nsm, st);
   if (rc == FMM_OK && mr > 0 && nd > 0)
-    rc = noalloc_launch(cp, terms, kUnitGrid, 1, A + md, lda, B, ldb, C + md, ldc, mr, nd, k, tickets, status, nsm,
-                        st);
+    rc = noalloc_launch(cp, terms, kUnitGrid, 1, A + md, lda, B, ldb, C + md, ldc, mr, nd, k, tickets, status,
+                        counter, nsm, st);
+  // The status word is not cleared per call: a timeout recorded by a sync = 0 call stays
+  // until a sync = 1 call or fmm_device_status() reports (and clears) it.
   if (rc == FMM_OK && sync) {
     unsigned v = 0;
     FMM_CUDA_TRY(cudaMemcpyAsync(&v, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     FMM_CUDA_TRY(cudaStreamSynchronize(st));
-    if (v) rc = FMM_E_TIMEOUT;
+    if (v) {
+      FMM_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
+      FMM_CUDA_TRY(cudaStreamSynchronize(st));
+      rc = FMM_E_TIMEOUT;
+    }
   }
   return rc;
 }
@@ -1463,12 +1706,14 @@ int split_core(const fmm_plan* plan, const DevTables& d, const float* A, long lo
   const size_t bytes_m = use_m ? sizeof(double) * (size_t)R * ms * ns : 0;
   const size_t bytes_t = (R > 1 && !use_m) ? sizeof(int) * (size_t)ntiles : 0;
   char* ws = nullptr;
-  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes_a + bytes_b + bytes_m + bytes_t + 16, st));
+  // planes, product tiles, then the work-unit counter and the tickets
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, bytes_a + bytes_b + bytes_m + sizeof(int) + bytes_t + 16, st));
   __nv_bfloat16* PA = reinterpret_cast<__nv_bfloat16*>(ws);
   __nv_bfloat16* PB = reinterpret_cast<__nv_bfloat16*>(ws + bytes_a);
   double* Mws = use_m ? reinterpret_cast<double*>(ws + bytes_a + bytes_b) : nullptr;
-  int* tickets = bytes_t ? reinterpret_cast<int*>(ws + bytes_a + bytes_b + bytes_m) : nullptr;
-  if (tickets) rc = cuda_status(cudaMemsetAsync(tickets, 0, bytes_t, st));
+  int* counter = reinterpret_cast<int*>(ws + bytes_a + bytes_b + bytes_m);
+  int* tickets = bytes_t ? counter + 1 : nullptr;
+  rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(int) + bytes_t, st));
 
   fmms::SplitArgs sa{};
   sa.X = A;
@@ -1516,6 +1761,7 @@ int split_core(const fmm_plan* plan, const DevTables& d, const float* A, long lo
     g.tiles_m = tiles_m;
     g.tiles_n = tiles_n;
     g.tickets = tickets;
+    g.counter = counter;
     g.M = Mws;
     g.ldm = ms;
     g.m_stride = (long long)ms * ns;
@@ -1618,7 +1864,7 @@ struct fmm_batch {
   fmm::GemmArgs* h_jobs[2] = {nullptr, nullptr};  // pinned staging of the job tables
   fmm::LincombTask* d_lc = nullptr;
   fmm::LincombTask* h_lc = nullptr;
-  int* d_tickets = nullptr;
+  int* d_tickets = nullptr;        // kBatchCounters work-unit counters (one per phase), then the tickets
   char* d_ws = nullptr;
   // Even-pitch copies of A / B for problems whose row count is odd (a dense operand then
   // has an odd leading dimension, which tensor copies cannot stage): byte offsets into
@@ -1819,7 +2065,7 @@ int batch_create(int count, const fmm_plan* const* plans, const int* m, const in
     e = cudaMalloc((void**)&b->d_lc, sizeof(fmm::LincombTask) * b->n_lincomb);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_lc, sizeof(fmm::LincombTask) * b->n_lincomb);
   }
-  if (e == cudaSuccess && b->n_tickets > 0) e = cudaMalloc((void**)&b->d_tickets, sizeof(int) * b->n_tickets);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_tickets, sizeof(int) * (kBatchCounters + b->n_tickets));
   if (e == cudaSuccess && b->ws_bytes > 0) e = cudaMalloc((void**)&b->d_ws, b->ws_bytes);
   if (e == cudaSuccess && b->pitch_bytes > 0) {
     e = cudaMalloc((void**)&b->d_pitch, b->pitch_bytes);
@@ -1856,7 +2102,7 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
     a.tiles_n = j.tiles_n;
     a.chunks = j.chunks;
     a.mode = fmm::MODE_ACCUM_C;
-    a.tickets = j.chunks > 1 ? b->d_tickets + j.ticket_off : nullptr;
+    a.tickets = j.chunks > 1 ? b->d_tickets + kBatchCounters + j.ticket_off : nullptr;
     a.status = dev_status[b->dev];
     const long long am = (long long)j.grid[0] * j.ms, ak = (long long)j.grid[1] * j.ks,
                     bn = (long long)j.grid[2] * j.ns;
@@ -1986,7 +2232,8 @@ void batch_prepare(fmm_batch* b, const double* const* A, const long* lda, const 
 
 // Enqueue the launches of a prepared batch whose tables are (being) copied to the device.
 int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool tma[2]) {
-  if (b->n_tickets > 0) FMM_CUDA_TRY(cudaMemsetAsync(b->d_tickets, 0, sizeof(int) * b->n_tickets, st));
+  // the phases' work-unit counters and every ticket start at zero
+  FMM_CUDA_TRY(cudaMemsetAsync(b->d_tickets, 0, sizeof(int) * (kBatchCounters + b->n_tickets), st));
   if (n_pc > 0) {
     ProfScope pf(K_PITCH_COPY, st);
     fmm::fmm_pitch_copy_kernel<<<dim3(256, (unsigned)n_pc), 256, 0, st>>>(b->d_pc);
@@ -2020,6 +2267,7 @@ int batch_launch(fmm_batch* b, cudaStream_t st, int n_lc, int n_pc, const bool t
     ba.njobs = (int)b->jobs[ph].size();
     ba.units = b->unit_start[ph].back();
     ba.status = dev_status[b->dev];
+    ba.counter = b->d_tickets + ph;
     const unsigned grid = (unsigned)std::min<long long>(ba.units, sm_count[b->dev]);
     {
       ProfScope pf(K_GEMM_BATCH, st);
@@ -2136,7 +2384,7 @@ int batch_submit(int count, const fmm_plan* const* plans, const int* m, const in
   off += sizeof(fmm::PitchCopy) * 2 * count;
   const size_t table_bytes = align_up(off, 256);
   const size_t o_tk = table_bytes;
-  const size_t o_ws = align_up(o_tk + sizeof(int) * b->n_tickets, 256);
+  const size_t o_ws = align_up(o_tk + sizeof(int) * (kBatchCounters + b->n_tickets), 256);
   const size_t o_pt = align_up(o_ws + b->ws_bytes, 256);
   const size_t dev_bytes = o_pt + b->pitch_bytes;
   char* stage = nullptr;
@@ -2159,7 +2407,7 @@ int batch_submit(int count, const fmm_plan* const* plans, const int* m, const in
   b->d_lc = reinterpret_cast<fmm::LincombTask*>(blk + o_lc);
   b->h_pc = reinterpret_cast<fmm::PitchCopy*>(stage + o_pc);
   b->d_pc = reinterpret_cast<fmm::PitchCopy*>(blk + o_pc);
-  b->d_tickets = b->n_tickets ? reinterpret_cast<int*>(blk + o_tk) : nullptr;
+  b->d_tickets = reinterpret_cast<int*>(blk + o_tk);
   b->d_ws = b->ws_bytes ? blk + o_ws : nullptr;
   b->d_pitch = b->pitch_bytes ? blk + o_pt : nullptr;
   int n_lc = 0, n_pc = 0;

@@ -71,8 +71,10 @@ constexpr unsigned TMA_BYTES_B8 = BN * BK * sizeof(double);    // direct B box
 static_assert((NSTAGE * STAGE_SZ * sizeof(double)) % 128 == 0, "raw slots must start 128-byte aligned");
 static_assert((TRAW_SZ * sizeof(double)) % 128 == 0, "TMA raw slots must be 128-byte aligned");
 static_assert((TRAW_A * sizeof(double)) % 128 == 0, "TMA B box must be 128-byte aligned");
-constexpr size_t SMEM_BYTES_CPASYNC =
-    (size_t)(NSTAGE * STAGE_SZ + NRAW * RAW_SZ) * sizeof(double) + 2 * NSTAGE * sizeof(unsigned long long);
+constexpr int UQ_DEPTH = 16;  // work-unit ring entries (see UnitClaimer)
+constexpr size_t RING_BYTES = 2 * UQ_DEPTH * sizeof(unsigned long long) + UQ_DEPTH * sizeof(int);
+constexpr size_t SMEM_BYTES_CPASYNC = (size_t)(NSTAGE * STAGE_SZ + NRAW * RAW_SZ) * sizeof(double) +
+                                      (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long) + RING_BYTES;
 // What the folding warps need to know about a raw slot, written by the issuer before
 // the slot's TMA copies (published by the release of its arrive.expect_tx).
 struct SlotMeta {
@@ -82,7 +84,7 @@ struct SlotMeta {
 };
 constexpr size_t SMEM_BYTES_TMA = (size_t)(NSTAGE * STAGE_SZ + NRAW_TMA * TRAW_SZ) * sizeof(double) +
                                   NRAW_TMA * sizeof(SlotMeta) +
-                                  (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long);
+                                  (2 * NSTAGE + 2 * NRAW_TMA) * sizeof(unsigned long long) + RING_BYTES;
 constexpr size_t smem_bytes(bool tma) { return tma ? SMEM_BYTES_TMA : SMEM_BYTES_CPASYNC; }
 constexpr int GROUP_M = 8;  // tile raster: groups of 8 tile rows for L2 reuse
 constexpr int C_BATCH_J = 4;          // epilogue: 8-column groups per batch of C loads (4 elements each);
@@ -115,7 +117,17 @@ struct Prod {
 
 enum Mode : int { MODE_ACCUM_C = 0, MODE_STORE_M = 1 };
 
+// STATUS_TICKET_TIMEOUT: a wait for another CTA's C updates gave up (the kernel finishes,
+// without the product order from then on); STATUS_WAIT_TIMEOUT: a wait inside a CTA's own
+// pipeline gave up (every later wait returns at once and the kernel winds down).
 enum StatusBits : unsigned { STATUS_TICKET_TIMEOUT = 1u, STATUS_WAIT_TIMEOUT = 2u };
+
+// Time limit of the bounded device-side waits in ns: WAIT_LIMIT_NS unless a test lowers it
+// (fmm_debug_set); read only on a wait's slow path.
+__device__ unsigned long long g_wait_limit_ns = WAIT_LIMIT_NS;
+__device__ __forceinline__ unsigned long long wait_limit_ns() {
+  return *reinterpret_cast<volatile unsigned long long*>(&g_wait_limit_ns);
+}
 
 struct GemmArgs {
   CUtensorMap tmA;   // whole-matrix tensor maps (TMA path), FP64: A (m x k), box BM x BK
@@ -149,6 +161,7 @@ struct GemmArgs {
   int nbt;          // > 0 (direct variant, one product per unit): tickets per (tile, C block),
   int nbc;          // nbt = C blocks, index tile * nbt + row * nbc + col, counting the block's
                     // updates in product order; 0: one ticket per tile
+  int* counter;     // work units claimed so far in this launch (zeroed before launch)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -209,20 +222,31 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Bounded wait for the phase with the given parity.  Every phase is completed by the
-// other warpgroup of the same CTA, so in a correct run the wait ends; if it has not
-// after WAIT_LIMIT_NS, the status word gets STATUS_WAIT_TIMEOUT and every later wait
-// of every CTA returns at once, so the kernel still finishes and the host reports
-// FMM_E_TIMEOUT.
+// Bounded wait for the phase with the given parity.  Every phase is completed by another
+// role of the same CTA, so in a correct run the wait ends; if it has not after the wait
+// limit, the status word gets STATUS_WAIT_TIMEOUT and every later such wait of every CTA
+// returns at once, so the kernel still finishes and the host reports FMM_E_TIMEOUT.  A
+// ticket timeout alone (STATUS_TICKET_TIMEOUT) does not cut these waits short: the
+// pipeline keeps running and every issued copy is consumed before the kernel ends.
 __device__ __forceinline__ void mbar_wait(unsigned bar, unsigned parity, unsigned* status) {
   if (mbar_try_wait(bar, parity)) return;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (*(volatile unsigned*)status != 0u) return;
-    if (global_ns() - t0 > WAIT_LIMIT_NS) {
+    if ((*(volatile unsigned*)status & STATUS_WAIT_TIMEOUT) != 0u) return;
+    if (global_ns() - t0 > wait_limit_ns()) {
       atomicOr(status, STATUS_WAIT_TIMEOUT);
       return;
     }
+  }
+}
+
+// Wait for a phase with a time limit only (no early exit on the status word): used at the
+// end of a role for copies that may still be in flight (only on an error path, where
+// other roles stopped consuming; in a normal run these phases have long completed).
+__device__ __forceinline__ void mbar_wait_drain(unsigned bar, unsigned parity) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > wait_limit_ns()) return;
   }
 }
 
@@ -239,6 +263,22 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
+// Bounded wait for a ticket written by another CTA: until *p >= target.  On timeout the
+// status word gets STATUS_TICKET_TIMEOUT; once any status bit is set, ticket waits return
+// at once.
+__device__ __forceinline__ void ticket_spin(const int* p, int target, unsigned* status, unsigned sleep_ns) {
+  if (ld_acquire(p) >= target) return;
+  const unsigned long long t0 = global_ns();
+  while (ld_acquire(p) < target) {
+    if (*(volatile unsigned*)status != 0u) return;
+    if (global_ns() - t0 > wait_limit_ns()) {
+      atomicOr(status, STATUS_TICKET_TIMEOUT);
+      return;
+    }
+    __nanosleep(sleep_ns);
+  }
+}
+
 __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2], double b) {
   asm volatile(
       "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
@@ -248,8 +288,8 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2]
 
 __device__ __forceinline__ int prod_T(const Prod& p) { return p.na > p.nb ? p.na : p.nb; }
 
-// Work unit u -> (tile position, product range).  Chunk-major order, so the units of
-// one tile are gridDim.x-strided apart and a later chunk starts well after the earlier.
+// Work unit u -> (tile position, product range).  Chunk-major order: the units of one tile
+// are a whole tile grid apart, so a later chunk is claimed well after the earlier one.
 struct Unit {
   int m0, n0, tile, r0, r1;
 };
@@ -288,6 +328,90 @@ __device__ __forceinline__ int num_units(const GemmArgs& a) {
 }
 
 // ------------------------------------------------------------------------------------
+// Work-unit claims.  One thread of each CTA (the operand issuer) claims the launch's units
+// in increasing order from a launch-wide counter and publishes each claimed index through
+// a shared-memory ring; every other role of the CTA reads the ring in the same order
+// (index -1 ends the sequence).  A unit waits only on tickets of lower-numbered units,
+// which running CTAs claimed before it, so the launch makes progress whether or not all of
+// its CTAs are resident at once (another kernel may hold some SMs).
+//
+// Ring depth: the issuer runs at most one operand pipeline (<= 6 stages of at least one
+// unit each) plus the product-tile hand-off ahead of the slowest reader, so 16 entries never
+// make it wait; if they did, the wait would end as the readers move on.
+// ------------------------------------------------------------------------------------
+struct UnitRing {
+  volatile int* slot;  // [UQ_DEPTH] in shared memory
+  unsigned full0;      // [UQ_DEPTH] barriers: entry published (1 arrival: the claimer)
+  unsigned empty0;     // [UQ_DEPTH] barriers: entry read by every reader warp
+};
+
+// The claiming thread: next unit index of this CTA, or -1 when the launch has none left.
+template <class Src>
+struct UnitClaimer {
+  const Src& src;
+  UnitRing q;
+  long long n = 0;
+  __device__ __forceinline__ int next() {
+    const int slot = (int)(n % UQ_DEPTH);
+    mbar_wait(q.empty0 + 8 * slot, (unsigned)(((n / UQ_DEPTH) & 1) ^ 1), src.status());
+    int u = -1;
+    if ((*(volatile unsigned*)src.status() & STATUS_WAIT_TIMEOUT) == 0u) {
+      u = atomicAdd(src.counter(), 1);
+      if (u >= src.total()) u = -1;
+    }
+    q.slot[slot] = u;
+    mbar_arrive(q.full0 + 8 * slot);  // release: the entry is visible to the readers' acquire
+    ++n;
+    return u;
+  }
+};
+
+// A reader warp (all 32 lanes call next() together), or a lone thread (lone = true) whose
+// warp has no other active lanes.  release = false reads an entry without freeing it (a
+// second cursor of the same warp frees it later).
+struct UnitReader {
+  UnitRing q;
+  unsigned* status;
+  bool release;
+  long long n = 0;
+  bool lone = false;
+  __device__ __forceinline__ int next() {
+    const int slot = (int)(n % UQ_DEPTH);
+    mbar_wait(q.full0 + 8 * slot, (unsigned)((n / UQ_DEPTH) & 1), status);
+    int u = q.slot[slot];
+    if ((*(volatile unsigned*)status & STATUS_WAIT_TIMEOUT) != 0u) u = -1;
+    if (release) {
+      if (lone) {
+        mbar_arrive(q.empty0 + 8 * slot);
+      } else {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(q.empty0 + 8 * slot);
+      }
+    }
+    ++n;
+    return u;
+  }
+};
+
+// Warp 0 of the per-thread-copy producer: lane 0 claims, the warp shares the index.
+template <class Src>
+struct WarpClaimer {
+  UnitClaimer<Src> c;
+  __device__ __forceinline__ int next() {
+    int u = 0;
+    if ((threadIdx.x & 31) == 0) u = c.next();
+    return __shfl_sync(0xffffffffu, u, 0);
+  }
+};
+
+__device__ __forceinline__ void unit_ring_init(const UnitRing& q, unsigned readers) {
+  for (int s = 0; s < UQ_DEPTH; ++s) {
+    mbar_init(q.full0 + 8 * s, 1);
+    mbar_init(q.empty0 + 8 * s, readers);
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // Producer: flattened stream of load units (k step s, term t) over the CTA's work units.
 // ------------------------------------------------------------------------------------
 struct LoadIter {
@@ -315,6 +439,7 @@ struct OneJob {
   __device__ __forceinline__ int first_unit(int) const { return 0; }
   __device__ __forceinline__ int total() const { return num_units(a); }
   __device__ __forceinline__ unsigned* status() const { return a.status; }
+  __device__ __forceinline__ int* counter() const { return a.counter; }
   __device__ __forceinline__ void acquire_maps(int) const {}
 };
 
@@ -323,6 +448,7 @@ struct JobBatch {
   const int* unit_start;
   int njobs, units;
   unsigned* st;
+  int* ctr;
   __device__ __forceinline__ const GemmArgs& get(int j) const { return jobs[j]; }
   __device__ __forceinline__ int find(int u) const {  // last j with unit_start[j] <= u
     int lo = 0, hi = njobs - 1;
@@ -338,6 +464,7 @@ struct JobBatch {
   __device__ __forceinline__ int first_unit(int j) const { return __ldg(unit_start + j); }
   __device__ __forceinline__ int total() const { return units; }
   __device__ __forceinline__ unsigned* status() const { return st; }
+  __device__ __forceinline__ int* counter() const { return ctr; }
   // The tensor maps were written into global memory by a copy before the launch; order
   // that write before the tensor-map proxy reads them.
   __device__ __forceinline__ void acquire_maps(int j) const {
@@ -367,15 +494,15 @@ __device__ __forceinline__ void iter_enter_unit(const Src& src, LoadIter& it) {
   load_terms(a, it);
 }
 
-template <class Src>
-__device__ __forceinline__ void load_iter_start(const Src& src, LoadIter& it) {
-  it.u = blockIdx.x;
-  it.valid = it.u < src.total();
+template <class Src, class Nx>
+__device__ __forceinline__ void load_iter_start(const Src& src, LoadIter& it, Nx& nx) {
+  it.u = nx.next();
+  it.valid = it.u >= 0;
   if (it.valid) iter_enter_unit(src, it);
 }
 
-template <class Src>
-__device__ __forceinline__ void load_iter_next(const Src& src, LoadIter& it) {
+template <class Src, class Nx>
+__device__ __forceinline__ void load_iter_next(const Src& src, LoadIter& it, Nx& nx) {
   const GemmArgs& a = src.get(it.j);
   if (++it.t < it.T) {
     load_terms(a, it);
@@ -393,8 +520,8 @@ __device__ __forceinline__ void load_iter_next(const Src& src, LoadIter& it) {
     load_terms(a, it);
     return;
   }
-  it.u += gridDim.x;
-  if (it.u >= src.total()) {
+  it.u = nx.next();
+  if (it.u < 0) {
     it.valid = false;
     return;
   }
@@ -494,18 +621,31 @@ __device__ __forceinline__ void fold_unit(const LoadIter& it, const double* raw_
   }
 }
 
+// The per-thread-copy producer's cursor that runs ahead (issuing copies): warp 0 claims the
+// units, the other producer warps read the ring without freeing entries; the trailing
+// cursor (folding) frees them.
+template <class Src>
+struct IssueCursor {
+  WarpClaimer<Src> c;
+  UnitReader r;
+  bool claim;  // warp-uniform
+  __device__ __forceinline__ int next() { return claim ? c.next() : r.next(); }
+};
+
 template <class Src>
 __device__ __forceinline__ void producer(const Src& src, double* stages, double* raw, unsigned full0, unsigned empty0,
-                                         int pt) {
+                                         int pt, const UnitRing& q) {
+  IssueCursor<Src> inx{WarpClaimer<Src>{UnitClaimer<Src>{src, q}}, UnitReader{q, src.status(), false}, pt < 32};
+  UnitReader cnx{q, src.status(), true};
   LoadIter iss, con;
-  load_iter_start(src, iss);
-  load_iter_start(src, con);
+  load_iter_start(src, iss, inx);
+  load_iter_start(src, con, cnx);
   // prologue: NRAW - 1 load units in flight
 #pragma unroll 1
   for (int i = 0; i < NRAW - 1; ++i) {
     if (iss.valid) {
       issue_unit(src.get(iss.j), iss, raw + (size_t)(i % NRAW) * RAW_SZ, pt);
-      load_iter_next(src, iss);
+      load_iter_next(src, iss, inx);
     }
     cp_async_commit();
   }
@@ -522,7 +662,7 @@ __device__ __forceinline__ void producer(const Src& src, double* stages, double*
     const bool last_term = (con.t == con.T - 1);
     if (iss.valid) {
       issue_unit(src.get(iss.j), iss, raw + (size_t)((unit + NRAW - 1) % NRAW) * RAW_SZ, pt);
-      load_iter_next(src, iss);
+      load_iter_next(src, iss, inx);
     }
     cp_async_commit();
     ++unit;
@@ -531,7 +671,7 @@ __device__ __forceinline__ void producer(const Src& src, double* stages, double*
       if ((pt & 31) == 0) mbar_arrive(full0 + 8 * stage);
       ++kc;
     }
-    load_iter_next(src, con);
+    load_iter_next(src, con, cnx);
   }
   cp_async_wait<0>();
 }
@@ -560,8 +700,8 @@ __device__ __forceinline__ KStep kstep_info(const GemmArgs& a, const LoadIter& i
 }
 
 // Per-k-step iterator over (unit, product, k step); ta / tb hold the first A / B term.
-template <class Src>
-__device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it) {
+template <class Src, class Nx>
+__device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it, Nx& nx) {
   it.t = 0;
   if (++it.s < it.nks) return;
   it.s = 0;
@@ -572,8 +712,8 @@ __device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it) {
     load_terms(a, it);
     return;
   }
-  it.u += gridDim.x;
-  if (it.u >= src.total()) {
+  it.u = nx.next();
+  if (it.u < 0) {
     it.valid = false;
     return;
   }
@@ -582,9 +722,10 @@ __device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it) {
 
 template <class Src>
 __device__ __forceinline__ void tma_issuer(const Src& src, double* stages, double* raw, SlotMeta* meta, unsigned full0,
-                                           unsigned empty0, unsigned rfull0, unsigned rempty0) {
+                                           unsigned empty0, unsigned rfull0, unsigned rempty0, const UnitRing& q) {
+  UnitClaimer<Src> nx{src, q};
   LoadIter it;
-  load_iter_start(src, it);
+  load_iter_start(src, it, nx);
   long long kc = 0, rc = 0;
   int mapped = -1;  // problem whose tensor maps were last acquired
 #pragma unroll 1
@@ -626,8 +767,11 @@ __device__ __forceinline__ void tma_issuer(const Src& src, double* stages, doubl
       if (hasB) tma_load_2d(smem_u32(rs + TRAW_A), tB.src ? &a.tmBw2 : &a.tmB2, xk & ~1, tB.col * a.ns + it.w.n0, rb);
     }
     ++kc;
-    kiter_next(src, it);
+    kiter_next(src, it, nx);
   }
+  // raw-slot copies still in flight (only on an error path) land before the CTA exits
+  for (long long q = rc - NRAW_TMA; q < rc; ++q)
+    if (q >= 0) mbar_wait_drain(rfull0 + 8 * (int)(q % NRAW_TMA), (unsigned)((q / NRAW_TMA) & 1));
 }
 
 // One raw slot folded into the running sums.  A: element pairs along m (16-byte
@@ -668,9 +812,11 @@ __device__ __forceinline__ void fold_slot(const double* rs, const SlotMeta& m, b
 
 template <class Src>
 __device__ __forceinline__ void tma_folder(const Src& src, double* stages, const double* raw, const SlotMeta* meta,
-                                           unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft) {
+                                           unsigned full0, unsigned empty0, unsigned rfull0, unsigned rempty0, int ft,
+                                           const UnitRing& q) {
+  UnitReader nx{q, src.status(), true};
   LoadIter it;
-  load_iter_start(src, it);
+  load_iter_start(src, it, nx);
   long long kc = 0, rc = 0;
   const int lane = ft & 31;
 #pragma unroll 1
@@ -727,7 +873,7 @@ __device__ __forceinline__ void tma_folder(const Src& src, double* stages, const
     __syncwarp();
     if (lane == 0) mbar_arrive(full0 + 8 * stage);
     ++kc;
-    kiter_next(src, it);
+    kiter_next(src, it, nx);
   }
 }
 
@@ -883,20 +1029,7 @@ __device__ __forceinline__ void prefetch_c_tiles(const GemmArgs& a, const Prod& 
 
 // Wait until the previous product chunk of this tile has finished its C updates.
 __device__ __forceinline__ void ticket_wait(const GemmArgs& a, int tile, int chunk, int ct) {
-  if (ct == 0) {
-    const int* tp = a.tickets + tile;
-    if (ld_acquire(tp) < chunk) {
-      const unsigned long long t0 = global_ns();
-      while (ld_acquire(tp) < chunk) {
-        if (*(volatile unsigned*)a.status != 0u) break;
-        if (global_ns() - t0 > WAIT_LIMIT_NS) {
-          atomicOr(a.status, STATUS_TICKET_TIMEOUT);
-          break;
-        }
-        __nanosleep(256);
-      }
-    }
-  }
+  if (ct == 0) ticket_spin(a.tickets + tile, chunk, a.status, 256);
   named_bar_sync(1, NCONS);
 }
 
@@ -908,15 +1041,15 @@ __device__ __forceinline__ void ticket_release(const GemmArgs& a, int tile, int 
 
 template <class Src>
 __device__ __forceinline__ void consumer(const Src& src, const double* stages, unsigned full0, unsigned empty0,
-                                         int ct) {
+                                         int ct, const UnitRing& q) {
   const int warp = ct >> 5, lane = ct & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
-  const int nunits = src.total();
+  UnitReader nx{q, src.status(), true};
   long long kc = 0;
   double acc[4][4][4];
 #pragma unroll 1
-  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+  for (int u = nx.next(); u >= 0; u = nx.next()) {
     const int job = src.find(u);
     const GemmArgs& a = src.get(job);
     const int ul = u - src.first_unit(job);
@@ -957,7 +1090,7 @@ __device__ __forceinline__ void consumer(const Src& src, const double* stages, u
   }
 }
 
-// Persistent: one CTA per SM walks work units blockIdx.x, blockIdx.x + gridDim.x, ...
+// Persistent: one CTA per SM takes work units in claim order (UnitClaimer) until none is left.
 // TMA = true stages operands with tensor copies (A, B 16-byte aligned, even leading
 // dimensions); TMA = false with per-thread cp.async (any alignment).
 template <bool TMA, class Src>
@@ -971,6 +1104,9 @@ __device__ __forceinline__ void gemm_cta(const Src& src) {
   const unsigned empty0 = smem_u32(bars + NSTAGE);
   const unsigned rfull0 = smem_u32(bars + 2 * NSTAGE);
   const unsigned rempty0 = smem_u32(bars + 2 * NSTAGE + NRAW_TMA);
+  unsigned long long* rbars = bars + 2 * NSTAGE + 2 * NRAW_TMA;
+  const UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * UQ_DEPTH), smem_u32(rbars),
+                   smem_u32(rbars + UQ_DEPTH)};
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
@@ -984,6 +1120,8 @@ __device__ __forceinline__ void gemm_cta(const Src& src) {
         mbar_init(rempty0 + 8 * s, NFOLD / 32);
       }
     }
+    // ring readers: folding + consumer warps (TMA); every producer and consumer warp (cp.async)
+    unit_ring_init(q, TMA ? (NFOLD + NCONS) / 32 : (NPROD + NCONS) / 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
@@ -991,15 +1129,15 @@ __device__ __forceinline__ void gemm_cta(const Src& src) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
     if (TMA) {
       if (tid == 0)
-        tma_issuer(src, stages, raw, meta, full0, empty0, rfull0, rempty0);
+        tma_issuer(src, stages, raw, meta, full0, empty0, rfull0, rempty0, q);
       else if (tid >= 32)
-        tma_folder(src, stages, raw, meta, full0, empty0, rfull0, rempty0, tid - 32);
+        tma_folder(src, stages, raw, meta, full0, empty0, rfull0, rempty0, tid - 32, q);
     } else {
-      producer(src, stages, raw, full0, empty0, tid);
+      producer(src, stages, raw, full0, empty0, tid, q);
     }
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
-    consumer(src, stages, full0, empty0, tid - NPROD);
+    consumer(src, stages, full0, empty0, tid - NPROD, q);
   }
 }
 
@@ -1017,11 +1155,12 @@ struct BatchArgs {
   int njobs;
   int units;
   unsigned* status;
+  int* counter;            // work units claimed so far (zeroed before launch)
 };
 
 template <bool TMA>
 __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_batch_kernel(const BatchArgs b) {
-  gemm_cta<TMA>(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status});
+  gemm_cta<TMA>(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status, b.counter});
 }
 
 // ------------------------------------------------------------------------------------
@@ -1037,13 +1176,15 @@ constexpr int NSTAGE_D = 4;
 constexpr int MS_LD = BM + 1;  // product tile in shared memory: column-major, padded
 constexpr int NEPI_D = NFOLD;  // epilogue threads (warps 1..7)
 static_assert((size_t)(NSTAGE_D * STAGE_SZ + BN * (BM + 1)) * sizeof(double) + 80 <= 232448, "direct variant shared memory");
-constexpr size_t SMEM_BYTES_DIRECT =
-    (size_t)(NSTAGE_D * STAGE_SZ + BN * MS_LD) * sizeof(double) + (2 * NSTAGE_D + 2) * sizeof(unsigned long long);
+constexpr size_t SMEM_BYTES_DIRECT = (size_t)(NSTAGE_D * STAGE_SZ + BN * MS_LD) * sizeof(double) +
+                                     (2 * NSTAGE_D + 2) * sizeof(unsigned long long) + RING_BYTES;
 
 template <class Src>
-__device__ __forceinline__ void direct_issuer(const Src& src, double* stages, unsigned full0, unsigned empty0) {
+__device__ __forceinline__ void direct_issuer(const Src& src, double* stages, unsigned full0, unsigned empty0,
+                                              const UnitRing& q) {
+  UnitClaimer<Src> nx{src, q};
   LoadIter it;
-  load_iter_start(src, it);
+  load_iter_start(src, it, nx);
   long long kc = 0;
   int mapped = -1;
 #pragma unroll 1
@@ -1063,21 +1204,25 @@ __device__ __forceinline__ void direct_issuer(const Src& src, double* stages, un
     tma_load_2d(smem_u32(opA + OPA_SZ), it.tb.src ? &a.tmBw : &a.tmB, it.tb.row * a.ks + k0,
                 it.tb.col * a.ns + it.w.n0, fb);
     ++kc;
-    kiter_next(src, it);
+    kiter_next(src, it, nx);
   }
+  // copies still in flight (only on an error path) land before the CTA exits
+  for (long long q = kc - NSTAGE_D; q < kc; ++q)
+    if (q >= 0) mbar_wait_drain(full0 + 8 * (int)(q % NSTAGE_D), (unsigned)((q / NSTAGE_D) & 1));
 }
 
 template <class Src>
 __device__ __forceinline__ void direct_consumer(const Src& src, const double* stages, double* Ms, unsigned full0,
-                                                unsigned empty0, unsigned mfull, unsigned mempty, int ct) {
+                                                unsigned empty0, unsigned mfull, unsigned mempty, int ct,
+                                                const UnitRing& uq) {
   const int warp = ct >> 5, lane = ct & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
-  const int nunits = src.total();
+  UnitReader nx{uq, src.status(), true};
   long long kc = 0, q = 0;
   double acc[4][4][4];
 #pragma unroll 1
-  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+  for (int u = nx.next(); u >= 0; u = nx.next()) {
     const int job = src.find(u);
     const GemmArgs& a = src.get(job);
     const int nks = (a.ks + BK - 1) / BK;
@@ -1127,13 +1272,13 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
 
 template <class Src>
 __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms, unsigned mfull, unsigned mempty,
-                                                int et) {
+                                                int et, const UnitRing& uq) {
   const int ew = et >> 5, lane = et & 31;
   constexpr int NW = NEPI_D / 32;  // 7 warps
-  const int nunits = src.total();
+  UnitReader nx{uq, src.status(), true};
   long long q = 0;
 #pragma unroll 1
-  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+  for (int u = nx.next(); u >= 0; u = nx.next()) {
     const int job = src.find(u);
     const GemmArgs& a = src.get(job);
     const int ul = u - src.first_unit(job);
@@ -1171,20 +1316,7 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
       }
       const bool per_block = ordered && a.nbt > 0;
       if (ordered && !per_block && r == w.r0) {
-        if (et == 0) {
-          const int* tp = a.tickets + w.tile;
-          if (ld_acquire(tp) < chunk) {
-            const unsigned long long t0 = global_ns();
-            while (ld_acquire(tp) < chunk) {
-              if (*(volatile unsigned*)a.status != 0u) break;
-              if (global_ns() - t0 > WAIT_LIMIT_NS) {
-                atomicOr(a.status, STATUS_TICKET_TIMEOUT);
-                break;
-              }
-              __nanosleep(256);
-            }
-          }
-        }
+        if (et == 0) ticket_spin(a.tickets + w.tile, chunk, a.status, 256);
         named_bar_sync(2, NEPI_D);
       }
       // C_l += w * M_r: warp ew takes columns ew, ew + 7, ... four at a time; a lane owns rows
@@ -1197,17 +1329,7 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
         int* tk = nullptr;
         if (per_block) {  // wait for the previous product that updates this C block
           tk = a.tickets + (long long)w.tile * a.nbt + tm.row * a.nbc + tm.col;
-          if (et == 0 && ld_acquire(tk) < tm.pad) {
-            const unsigned long long t0 = global_ns();
-            while (ld_acquire(tk) < tm.pad) {
-              if (*(volatile unsigned*)a.status != 0u) break;
-              if (global_ns() - t0 > WAIT_LIMIT_NS) {
-                atomicOr(a.status, STATUS_TICKET_TIMEOUT);
-                break;
-              }
-              __nanosleep(128);
-            }
-          }
+          if (et == 0) ticket_spin(tk, tm.pad, a.status, 128);
           named_bar_sync(2, NEPI_D);
         }
         double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc + w.m0 + lane;
@@ -1261,6 +1383,9 @@ __device__ __forceinline__ void gemm_cta_direct(const Src& src) {
   const unsigned empty0 = smem_u32(bars + NSTAGE_D);
   const unsigned mfull = smem_u32(bars + 2 * NSTAGE_D);
   const unsigned mempty = smem_u32(bars + 2 * NSTAGE_D + 1);
+  unsigned long long* rbars = bars + 2 * NSTAGE_D + 2;
+  const UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * UQ_DEPTH), smem_u32(rbars),
+                   smem_u32(rbars + UQ_DEPTH)};
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE_D; ++s) {
@@ -1269,18 +1394,19 @@ __device__ __forceinline__ void gemm_cta_direct(const Src& src) {
     }
     mbar_init(mfull, NCONS / 32);
     mbar_init(mempty, NEPI_D / 32);
+    unit_ring_init(q, (NEPI_D + NCONS) / 32);  // ring readers: epilogue + consumer warps
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
   if (tid < NPROD) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PROD_REGS));
     if (tid == 0)
-      direct_issuer(src, stages, full0, empty0);
+      direct_issuer(src, stages, full0, empty0, q);
     else if (tid >= 32)
-      direct_epilogue(src, Ms, mfull, mempty, tid - 32);
+      direct_epilogue(src, Ms, mfull, mempty, tid - 32, q);
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONS_REGS));
-    direct_consumer(src, stages, Ms, full0, empty0, mfull, mempty, tid - NPROD);
+    direct_consumer(src, stages, Ms, full0, empty0, mfull, mempty, tid - NPROD, q);
   }
 }
 
@@ -1289,7 +1415,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_direct_kernel(const __gr
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1) fmm_gemm_direct_batch_kernel(const BatchArgs b) {
-  gemm_cta_direct(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status});
+  gemm_cta_direct(JobBatch{b.jobs, b.unit_start, b.njobs, b.units, b.status, b.counter});
 }
 
 // Operand sums in HBM: out_j = sum_t coef_t * X_{blk_t} for the A terms (side 0) or the

@@ -17,9 +17,10 @@
 //      products the epilogue stores M_r (FP64) to a workspace and fmm_combine_kernel adds
 //      W[l,r] * M_r into C afterwards; a single product is added into C directly.
 //
-// Work unit = (128 x 128 tile position, product r); a unit owns its tile position in every
-// C block, and per-tile tickets order the products' C updates (no atomics on C, the result
-// does not depend on scheduling).  Warp roles (384 threads, one CTA per SM, persistent):
+// Work unit = (128 x 128 tile position, product r), claimed in order from a launch-wide
+// counter (fmm::UnitClaimer); a unit owns its tile position in every C block, and per-tile
+// tickets order the products' C updates (no atomics on C, the result does not depend on
+// scheduling).  Warp roles (384 threads, one CTA per SM, persistent):
 // warp 0 lane 0 issues TMA (128-byte swizzle, each CTA loads its own tiles), warp 1 owns tensor memory and
 // its lane 0 issues the MMAs, warps 4..11 drain the accumulator and run the epilogue.
 // Every wait is bounded; tensor memory is freed on every path.
@@ -55,7 +56,8 @@ constexpr int NTHREADS = 384;
 constexpr int NEPI = 256;                                // epilogue threads (warps 4..11)
 constexpr int KPAD = 64;                                 // plane row pitch multiple
 constexpr int NBARS = 2 * NSTG + 2 * NACC + 1;
-constexpr size_t SMEM_BYTES = (size_t)NSTG * STAGE_BYTES + 1024 /*alignment slack*/ + 8 * NBARS + 16;
+constexpr size_t SMEM_BYTES =
+    (size_t)NSTG * STAGE_BYTES + 1024 /*alignment slack*/ + 8 * NBARS + 16 /*tensor-memory address*/ + fmm::RING_BYTES;
 constexpr int GROUP_M = 8;
 constexpr int DRAIN_STAGES = 2;                          // stages (of BK) accumulated in FP32 before each FP64 drain
 constexpr int C_PREFETCH_CHUNKS = 4;                     // C tiles go to L2 this many drains before a unit ends
@@ -81,6 +83,15 @@ struct SplitGemmArgs {
   long long ldm;     // of being added into C; a combine pass applies W afterwards
   long long m_stride;
   unsigned* status;
+  int* counter;      // work units claimed so far (zeroed before launch)
+};
+
+// Where the split kernel's work units come from (for fmm::UnitClaimer).
+struct SplitSrc {
+  const SplitGemmArgs& a;
+  __device__ __forceinline__ int total() const { return a.tiles_m * a.tiles_n * a.nprod; }
+  __device__ __forceinline__ unsigned* status() const { return a.status; }
+  __device__ __forceinline__ int* counter() const { return a.counter; }
 };
 
 // UMMA shared-memory descriptor of a K-major operand tile stored with the 128-byte
@@ -134,14 +145,7 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&r)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-// Wait for a phase with a time limit only (no early exit on the status word): used at
-// the end of the kernel for copies and MMAs that may still be in flight.
-__device__ __forceinline__ void mbar_wait_drain(unsigned bar, unsigned parity) {
-  const unsigned long long t0 = fmm::global_ns();
-  while (!fmm::mbar_try_wait(bar, parity)) {
-    if (fmm::global_ns() - t0 > fmm::WAIT_LIMIT_NS) return;
-  }
-}
+using fmm::mbar_wait_drain;  // time-limited wait for copies and MMAs still in flight at the end
 
 // The unit's C tiles (every C block of product p) into L2: 128-byte lines of 16 rows of
 // one column, spread over the epilogue threads.
@@ -190,9 +194,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
   const unsigned acce0 = fmm::smem_u32(bars + 2 * NSTG + NACC);  // [NACC] chunk drained
   const unsigned done_bar = fmm::smem_u32(bars + 2 * NSTG + 2 * NACC);  // every MMA complete
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + NBARS);
+  unsigned long long* rbars = bars + NBARS + 2;
+  const fmm::UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * fmm::UQ_DEPTH), fmm::smem_u32(rbars),
+                        fmm::smem_u32(rbars + fmm::UQ_DEPTH)};
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nks = a.kpad / BK;
-  const int nunits = a.tiles_m * a.tiles_n * a.nprod;
 
   if (tid == 0) {
     for (int s = 0; s < NSTG; ++s) {
@@ -204,6 +210,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
       fmm::mbar_init(acce0 + 8 * b, NEPI / 32);
     }
     fmm::mbar_init(done_bar, 1);
+    fmm::unit_ring_init(q, 1 + NEPI / 32);  // ring readers: the MMA thread and the epilogue warps
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 1) {
@@ -219,9 +226,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
 
   if (warp == 0) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(CTL_REGS));
-    if (lane == 0) {  // ---- TMA producer ----
+    if (lane == 0) {  // ---- TMA producer; claims the work units ----
+      const SplitSrc src{a};
+      fmm::UnitClaimer<SplitSrc> nx{src, q};
       long long kc = 0;
-      for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      for (int u = nx.next(); u >= 0; u = nx.next()) {
         const SUnit w = s_decode(a, u);
         const int ya = 3 * w.r * a.ms + w.m0, yb = 3 * w.r * a.ns + w.n0;
         for (int s = 0; s < nks; ++s, ++kc) {
@@ -248,8 +257,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
       // plane pairs (A plane, B plane); the last, hi*hi, has an accumulator of its own
       constexpr int pa[NPAIR] = {2, 0, 1, 1, 0, 0};
       constexpr int pb[NPAIR] = {0, 2, 1, 0, 1, 0};
+      fmm::UnitReader nx{q, a.status, true, 0, true};
       long long kc = 0, ch = 0;
-      for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+      for (int u = nx.next(); u >= 0; u = nx.next()) {
         for (int s = 0; s < nks; ++s, ++kc) {
           const int stg = (int)(kc % NSTG);
           const int b = (int)(ch % NACC);
@@ -289,8 +299,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
     const int quarter = warp & 3, half = (warp - 4) >> 2;
     const int row = quarter * 32 + lane;
     const bool ordered = a.nprod > 1 && a.M == nullptr;
+    fmm::UnitReader nx{q, a.status, true};
     long long ch = 0;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    for (int u = nx.next(); u >= 0; u = nx.next()) {
       const SUnit w = s_decode(a, u);
       double acc[64];
 #pragma unroll
@@ -330,20 +341,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
       }
       // this tile position's updates from products < r are complete
       if (ordered && w.r > 0) {
-        if (et == 0) {
-          const int* tp = a.tickets + w.tile;
-          if (fmm::ld_acquire(tp) < w.r) {
-            const unsigned long long t0 = fmm::global_ns();
-            while (fmm::ld_acquire(tp) < w.r) {
-              if (*(volatile unsigned*)a.status != 0u) break;
-              if (fmm::global_ns() - t0 > fmm::WAIT_LIMIT_NS) {
-                atomicOr(a.status, fmm::STATUS_TICKET_TIMEOUT);
-                break;
-              }
-              __nanosleep(256);
-            }
-          }
-        }
+        if (et == 0) fmm::ticket_spin(a.tickets + w.tile, w.r, a.status, 256);
         fmm::named_bar_sync(1, NEPI);
       }
       // C_l += W[l, r] * M_r in FP64; a warp's lanes cover 32 consecutive rows of a column

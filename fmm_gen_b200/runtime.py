@@ -121,6 +121,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_profile_num_kinds.restype = c_int
     lib.fmm_profile_kind_name.argtypes = [c_int]
     lib.fmm_profile_kind_name.restype = ctypes.c_char_p
+    lib.fmm_device_status.argtypes = [c_int]
+    lib.fmm_device_status.restype = c_int
+    lib.fmm_debug_set.argtypes = [c_int, ctypes.c_longlong]
+    lib.fmm_debug_set.restype = c_int
 
 
 def _check(rc: int, what: str) -> None:

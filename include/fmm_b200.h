@@ -102,25 +102,44 @@ int fmm_dgemm_host(const fmm_plan *plan, int pack_type, int m, int n, int k, con
 
 /* Device-side status of the current device: FMM_E_TIMEOUT if a bounded wait inside a
  * kernel gave up since the last clear (results of that call are then unreliable),
- * FMM_OK otherwise.  Synchronises with the device; clear != 0 resets the word.  The
+ * FMM_OK otherwise.  Covers every entry point, fmm_dgemm_dev_noalloc's status word
+ * included.  Synchronises with the device; clear != 0 resets the words.  The
  * synchronous host entry points check it themselves. */
 int fmm_device_status(int clear);
+
+/* Test hooks -- no counterpart in the reference, whose code has no device-side waits.
+ *   FMM_DEBUG_WAIT_LIMIT_NS: time limit of every bounded device-side wait on the current
+ *     device, in ns (default 4e9; value <= 0 restores the default).
+ *   FMM_DEBUG_TICKET_FILL: byte written into every ticket of a single-problem FMM launch
+ *     before it runs (default 0).  0xFF starts every ticket at -1, which no launch ever
+ *     releases, so the launch's first ticket waits run out: the kernel records
+ *     FMM_E_TIMEOUT after the limit, stops waiting for tickets, and finishes (its result
+ *     is then unreliable); fmm_device_status() reports it.  Lets a test check the
+ *     timeout path without a fault.
+ * Process-wide settings for tests; restore both before other work.  FMM_E_INVALID for an
+ * unknown setting or a fill outside 0..255. */
+#define FMM_DEBUG_WAIT_LIMIT_NS 1
+#define FMM_DEBUG_TICKET_FILL 2
+int fmm_debug_set(int what, long long value);
 
 /* FMM C += A*B (pack type ABC) that allocates no memory -- no counterpart in the
  * reference.  For callers that cannot allocate device memory at call time: frameworks
  * that own all device memory through their own arena or caching allocator, and
  * latency-critical paths where an allocation is not acceptable.  Operand sums are
- * folded while staging (no workspace); the only scratch -- per-tile tickets, a status
- * word and the plan's tables -- lives in one statically allocated device array (about
+ * folded while staging (no workspace); the only scratch -- per-tile tickets, a work-unit
+ * counter, a status word and the plan's tables -- lives in one statically allocated device array (about
  * 384 KB, held by every GPU that loads the library until the process exits).
  *   Limits: plan with <= 1024 products and <= 12288 terms; <= 16384 tiles of 128 x 128
  *   in a product (ms x ns); beyond them it returns FMM_E_TOO_LARGE without running.
- *   The first call on a device resolves the array's address (cudaGetSymbolAddress) and
- *   configures the kernels; make that first call before any stream capture.
+ *   The first call on a device resolves the array's address (cudaGetSymbolAddress),
+ *   configures the kernels and writes the fringe strips' constant tables and a zero
+ *   status word with blocking copies; make that first call before any stream capture.
  *   Every call shares the array: calls that overlap on the GPU (other streams, other
  *   host threads) race; serialise them on one stream.
  *   sync != 0: synchronise the stream and report a device-side wait timeout
- *   (FMM_E_TIMEOUT); sync == 0: stream-ordered, launch errors only. */
+ *   (FMM_E_TIMEOUT, then the word is cleared); sync == 0: stream-ordered, launch errors
+ *   only -- a timeout stays recorded in the status word until a sync != 0 call or
+ *   fmm_device_status() reports it. */
 int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const double *A, long lda, const double *B,
                           long ldb, double *C, long ldc, void *stream, int sync);
 

@@ -70,15 +70,44 @@ def bl_dgemm(A, B, C) -> None:
     load().oracle_bl_dgemm(m, n, k, _p(_cm(A)), max(m, 1), _p(_cm(B)), max(k, 1), _p(_cm(C)), max(m, 1))
 
 
+def _ld(x: np.ndarray) -> int:
+    """Leading dimension of a float64 column-major array or of a column-major view of one
+    (unit row stride), e.g. A[:md, :kd] of a Fortran array."""
+    if x.dtype != np.float64 or x.ndim != 2 or (x.shape[0] > 1 and x.strides[0] != 8) or x.strides[1] % 8:
+        raise ValueError("oracle arrays must be float64, column-major (unit row stride)")
+    return max(x.strides[1] // 8, x.shape[0], 1)
+
+
 def fmm(tables, pack: str, A, B, C) -> None:
-    """FMM C += A @ B; `tables` = (dims, R, nterms, rows, cols, coefs) as int32/float64 arrays."""
+    """FMM C += A @ B; `tables` = (dims, R, nterms, rows, cols, coefs) as int32/float64 arrays.
+    A, B, C are Fortran arrays or column-major views of them (their leading dimensions are
+    passed on)."""
     dims, R, nterms, rows, cols, coefs = tables
     m, k = A.shape
     n = B.shape[1]
     rc = load().oracle_fmm(PACKS[pack], _p(dims), int(R), _p(nterms), _p(rows), _p(cols), _p(coefs), m, n, k,
-                           _p(_cm(A)), max(m, 1), _p(_cm(B)), max(k, 1), _p(_cm(C)), max(m, 1))
+                           _p(A), _ld(A), _p(B), _ld(B), _p(C), _ld(C))
     if rc:
         raise RuntimeError(f"oracle_fmm failed: {rc}")
+
+
+def dynamic_peeling(A, B, C, d1: int, d2: int, d3: int) -> None:
+    """The fringe strips of an FMM call (the reference's bl_dynamic_peeling), in place."""
+    m, k = A.shape
+    n = B.shape[1]
+    load().oracle_dynamic_peeling(m, n, k, _p(A), _ld(A), _p(B), _ld(B), _p(C), _ld(C), d1, d2, d3)
+
+
+def product_subset(tables, prods):
+    """Plan tables restricted to the products `prods` (in that order): used to time a sample
+    of a large call's products."""
+    dims, R, nterms, rows, cols, coefs = tables
+    nt = np.asarray(nterms, dtype=np.int32).reshape(R, 3)
+    starts = np.concatenate([[0], np.cumsum(nt.sum(axis=1))])
+    sel = np.concatenate([np.arange(starts[r], starts[r + 1]) for r in prods])
+    return (dims, len(prods), np.ascontiguousarray(nt[list(prods)].reshape(-1)),
+            np.ascontiguousarray(rows[sel], dtype=np.int32), np.ascontiguousarray(cols[sel], dtype=np.int32),
+            np.ascontiguousarray(coefs[sel], dtype=np.float64))
 
 
 def dgemm_dot2(A, B, C) -> None:

@@ -1,8 +1,8 @@
 """Generate the golden fixtures that pin the oracle and the algebra layer to fmm-gen.
 
-Run in a container that has the fmm-gen checkout (default /root/reference, override
-with FMM_REF); the fixtures it writes next to this file are committed, so the tests
-never read the checkout.
+Run where an fmm-gen checkout exists, named by the environment variable FMM_REF (no
+default); the fixtures it writes next to this file are committed, so the tests never
+read the checkout.
 
 What it does:
   1. Loads the reference's Python 2 generator modules (meta/*.py) into memory with a
@@ -23,7 +23,7 @@ What it does:
      (meta/abc_micro_kernel_gen.py:1104-1108), so it does not compile when a product
      updates two or more C blocks; the missing commas are inserted.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  FMM_REF=<fmm-gen checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -39,7 +39,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FMM_REF", "/root/reference")
+REF = os.environ.get("FMM_REF", "")
 META = os.path.join(REF, "meta")
 ALGS = os.path.join(META, "algorithms")
 
@@ -264,6 +264,8 @@ def main():
         _, _, lib, fn, shapes, seed0, out = sys.argv
         _child(lib, fn, json.loads(shapes), int(seed0), out)
         return
+    if not REF or not os.path.isdir(META):
+        sys.exit("set FMM_REF to an fmm-gen checkout (the directory that holds meta/ and common/)")
     os.environ["BLISLAB_IC_NT"] = "1"
     os.environ["OMP_NUM_THREADS"] = "1"
     mods = load_reference()

@@ -306,3 +306,33 @@ def test_gpu_plain_k_tail(oracle_lib, m, n, k):
     want = C.copy(order="F")
     oracle_lib.bl_dgemm(A, B, want)
     assert rel_fro(got, want) <= RTOL_SMALL
+
+
+# Launches of few work units split every product's k range (k-split tables): the parts'
+# C updates, in order under the same tickets, add up to the product.  These shapes take
+# S = 4 (plain 2048^3: 256 tiles on 148 SMs), S = 8 (plain 1024 x 2048 x 4096) and S > 1
+# for 222-1 (2048^3: 448 units, pre-summed operands).
+KSPLIT_CASES = [
+    (None, (2048, 2048, 2048)),
+    (None, (1024, 2048, 4096)),
+    ((["222"], [1]), (2048, 2048, 2048)),
+    ((["222"], [1]), (2048, 1536, 4096)),
+]
+
+
+@pytest.mark.parametrize("algo,shape", KSPLIT_CASES, ids=lambda x: str(x))
+def test_gpu_ksplit_matches_oracle(oracle_lib, algo, shape):
+    m, n, k = shape
+    A, B, C = inputs(m + 2 * n + 5 * k, m, n, k)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    want = C.copy(order="F")
+    if algo is None:
+        rt.plain_gemm(dA, dB, dC)
+        oracle_lib.bl_dgemm(A, B, want)
+    else:
+        p = plan_for(*algo)
+        rt.fmm_gemm(p, dA, dB, dC, "abc")
+        oracle_lib.fmm(tables(p.algebra), "abc", A, B, want)
+    torch.cuda.synchronize()
+    assert rt.load_library().fmm_device_status(1) == 0
+    assert rel_fro(dC.cpu().numpy(), want) <= RTOL_SMALL

@@ -67,6 +67,46 @@ def test_noalloc_matches_regular_entry_point_twice(lib, algs, levels, shape):
     assert (got - want).abs().max().item() <= 4 * bound
 
 
+@pytest.mark.parametrize("algs,levels,shape", [
+    (["222"], [1], (15, 9, 300)),                 # fringe only: m below the plan's block multiple (md = 0)
+    (["333"], [1], (300, 260, 2)),                # fringe only: k below the plan's k split (kd = 0)
+    (None, None, (517, 389, 263)),                # classical 1 x 1 x 1 plan
+])
+def test_noalloc_fringe_only_and_classical(lib, algs, levels, shape):
+    m, n, k = shape
+    plan = rt.Plan(algebra.classical_plan()) if algs is None else rt.Plan.from_levels(algs, levels)
+    g = torch.Generator(device="cuda").manual_seed(3 * m + n + k)
+    A, B, C0 = _rand(m, k, g), _rand(k, n, g), _rand(m, n, g)
+    stream = torch.cuda.current_stream()
+    got = rt.colmajor(m, n, device="cuda").copy_(C0)
+    want = rt.colmajor(m, n, device="cuda").copy_(C0)
+    for _ in range(2):
+        assert _noalloc(lib, plan, A, B, got, stream) == 0
+        rt.fmm_gemm(plan, A, B, want, "abc")
+    torch.cuda.synchronize()
+    assert ((got - want).norm() / want.norm()).item() <= RTOL
+
+
+def test_noalloc_back_to_back_without_sync(lib):
+    """Two sync = 0 calls on one stream reuse the scratch before the host synchronises; one
+    stream synchronisation afterwards, then the status reads clean."""
+    m, n, k = 1000, 900, 700
+    plan = rt.Plan.from_levels(["222", "333"], [1, 1])
+    g = torch.Generator(device="cuda").manual_seed(77)
+    A, B, C0 = _rand(m, k, g), _rand(k, n, g), _rand(m, n, g)
+    stream = torch.cuda.current_stream()
+    got = rt.colmajor(m, n, device="cuda").copy_(C0)
+    want = rt.colmajor(m, n, device="cuda").copy_(C0)
+    assert _noalloc(lib, plan, A, B, got, stream, sync=0) == 0
+    assert _noalloc(lib, plan, A, B, got, stream, sync=0) == 0
+    stream.synchronize()
+    assert lib.fmm_device_status(1) == 0
+    for _ in range(2):
+        rt.fmm_gemm(plan, A, B, want, "abc")
+    torch.cuda.synchronize()
+    assert ((got - want).norm() / want.norm()).item() <= RTOL
+
+
 def test_noalloc_rejects_sizes_beyond_its_limits(lib):
     plan = rt.Plan.from_levels(["222"], [1])
     m = n = 2 * 16512  # ms = ns = 16512 -> 129 x 129 = 16641 tiles
