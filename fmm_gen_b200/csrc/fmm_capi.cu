@@ -577,13 +577,15 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
   const long long am = (long long)grid_dims[0] * ms, ak = (long long)grid_dims[1] * (ks_orig >= 0 ? ks_orig : ks),
                   bn = (long long)grid_dims[2] * ns;
   bool tma = make_tensor_map(&a.tmA, A, am, ak, lda, fmm::BM, fmm::BK) &&
+             make_tensor_map(&a.tmA64, A, am, ak, lda, fmm::BM / 2, fmm::BK) &&
              make_tensor_map(&a.tmB, B, ak, bn, ldb, fmm::BK, fmm::BN) &&
              make_tensor_map(&a.tmB2, B, ak, bn, ldb, fmm::TB_K, fmm::BN);
   if (tma) {
     if (ps.S && ps.nslotA > 0)
-      tma = make_tensor_map(&a.tmAw, ps.S, ms, (long long)ps.nslotA * ks, ps.ldS, fmm::BM, fmm::BK);
+      tma = make_tensor_map(&a.tmAw, ps.S, ms, (long long)ps.nslotA * ks, ps.ldS, fmm::BM, fmm::BK) &&
+            make_tensor_map(&a.tmAw64, ps.S, ms, (long long)ps.nslotA * ks, ps.ldS, fmm::BM / 2, fmm::BK);
     else
-      a.tmAw = a.tmA;
+      a.tmAw = a.tmA, a.tmAw64 = a.tmA64;
   }
   if (tma) {
     if (ps.T && ps.nslotB > 0)
@@ -2147,12 +2149,14 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
       a.ldbw = lb;
     }
     bool ok = make_tensor_map(&a.tmA, a.A, am, ak, la, fmm::BM, fmm::BK) &&
+              make_tensor_map(&a.tmA64, a.A, am, ak, la, fmm::BM / 2, fmm::BK) &&
               make_tensor_map(&a.tmB, a.B, ak, bn, lb, fmm::BK, fmm::BN) &&
               make_tensor_map(&a.tmB2, a.B, ak, bn, lb, fmm::TB_K, fmm::BN);
     if (ok && j.presum && j.nA > 0)
-      ok = make_tensor_map(&a.tmAw, a.Aw, j.ms, (long long)j.nA * j.kk, j.ms, fmm::BM, fmm::BK);
+      ok = make_tensor_map(&a.tmAw, a.Aw, j.ms, (long long)j.nA * j.kk, j.ms, fmm::BM, fmm::BK) &&
+           make_tensor_map(&a.tmAw64, a.Aw, j.ms, (long long)j.nA * j.kk, j.ms, fmm::BM / 2, fmm::BK);
     else
-      a.tmAw = a.tmA;
+      a.tmAw = a.tmA, a.tmAw64 = a.tmA64;
     if (ok && j.presum && j.nB > 0)
       ok = make_tensor_map(&a.tmBw, a.Bw, j.kk, (long long)j.nB * j.ns, j.ldT, fmm::BK, fmm::BN) &&
            make_tensor_map(&a.tmBw2, a.Bw, j.kk, (long long)j.nB * j.ns, j.ldT, fmm::TB_K, fmm::BN);

@@ -136,6 +136,8 @@ struct GemmArgs {
   CUtensorMap tmAw;  // the same three for the pre-summed workspaces S (A side) and T (B side)
   CUtensorMap tmBw;
   CUtensorMap tmBw2;
+  CUtensorMap tmA64;   // A and S again with a box of BM / 2 rows: the half-height units of the
+  CUtensorMap tmAw64;  // direct variant (see Unit)
   const double* A;
   long long lda;
   const double* B;
@@ -162,6 +164,7 @@ struct GemmArgs {
   int nbc;          // nbt = C blocks, index tile * nbt + row * nbc + col, counting the block's
                     // updates in product order; 0: one ticket per tile
   int* counter;     // work units claimed so far in this launch (zeroed before launch)
+  int bm;           // tile height: BM, or BM / 2 (direct variant only); 0 means BM
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -290,10 +293,22 @@ __device__ __forceinline__ int prod_T(const Prod& p) { return p.na > p.nb ? p.na
 
 // Work unit u -> (tile position, product range).  Chunk-major order: the units of one tile
 // are a whole tile grid apart, so a later chunk is claimed well after the earlier one.
+// rows: the tile's rows inside the block (at most the tile height).  half: the tile has at
+// most BM / 2 rows (a job of half-height tiles, or the last tile row of a block whose height
+// leaves <= 64 rows there); the direct variant then stages a BM / 2-row box of A and lets
+// both rows of consumer warps cover those rows, taking alternate k steps.
 struct Unit {
   int m0, n0, tile, r0, r1;
 };
 
+__device__ __forceinline__ int tile_height(const GemmArgs& a) { return a.bm > 0 ? a.bm : BM; }
+// rows of the unit's tile inside the block, and whether that makes it a half-height unit
+__device__ __forceinline__ int unit_rows(const GemmArgs& a, const Unit& w) { return min(tile_height(a), a.ms - w.m0); }
+__device__ __forceinline__ bool unit_half(const GemmArgs& a, const Unit& w) { return unit_rows(a, w) <= BM / 2; }
+
+// VARH: the job's tile height may be BM / 2 (direct variant); the other kernels use BM, known
+// at compile time.
+template <bool VARH = false>
 __device__ __forceinline__ Unit decode_unit(const GemmArgs& a, int u) {
   const int ntiles = a.tiles_m * a.tiles_n;
   Unit w;
@@ -316,7 +331,7 @@ __device__ __forceinline__ Unit decode_unit(const GemmArgs& a, int u) {
   const int in_grp = bid % per_group;
   const int tile_m = first_m + in_grp % rows_here;
   const int tile_n = in_grp / rows_here;
-  w.m0 = tile_m * BM;
+  w.m0 = tile_m * (VARH ? tile_height(a) : BM);
   w.n0 = tile_n * BN;
   w.tile = bid;
   return w;
@@ -340,27 +355,39 @@ __device__ __forceinline__ int num_units(const GemmArgs& a) {
 // make it wait; if they did, the wait would end as the readers move on.
 // ------------------------------------------------------------------------------------
 struct UnitRing {
-  volatile int* slot;  // [UQ_DEPTH] in shared memory
-  unsigned full0;      // [UQ_DEPTH] barriers: entry published (1 arrival: the claimer)
-  unsigned empty0;     // [UQ_DEPTH] barriers: entry read by every reader warp
+  unsigned base;  // shared address: UQ_DEPTH full barriers (entry published: 1 arrival, the
+                  // claimer), UQ_DEPTH empty barriers (entry read by every reader warp), then
+                  // UQ_DEPTH int entries
+  __device__ __forceinline__ unsigned full(int s) const { return base + 8 * s; }
+  __device__ __forceinline__ unsigned empty(int s) const { return base + 8 * (UQ_DEPTH + s); }
+  __device__ __forceinline__ unsigned entry(int s) const { return base + 16 * UQ_DEPTH + 4 * s; }
 };
+
+__device__ __forceinline__ void st_shared_s32(unsigned addr, int v) {
+  asm volatile("st.shared.s32 [%0], %1;\n" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_shared_s32(unsigned addr) {
+  int v;
+  asm volatile("ld.shared.s32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
 
 // The claiming thread: next unit index of this CTA, or -1 when the launch has none left.
 template <class Src>
 struct UnitClaimer {
   const Src& src;
   UnitRing q;
-  long long n = 0;
+  int n = 0;
   __device__ __forceinline__ int next() {
-    const int slot = (int)(n % UQ_DEPTH);
-    mbar_wait(q.empty0 + 8 * slot, (unsigned)(((n / UQ_DEPTH) & 1) ^ 1), src.status());
+    const int slot = n % UQ_DEPTH;
+    mbar_wait(q.empty(slot), (unsigned)(((n / UQ_DEPTH) & 1) ^ 1), src.status());
     int u = -1;
     if ((*(volatile unsigned*)src.status() & STATUS_WAIT_TIMEOUT) == 0u) {
       u = atomicAdd(src.counter(), 1);
       if (u >= src.total()) u = -1;
     }
-    q.slot[slot] = u;
-    mbar_arrive(q.full0 + 8 * slot);  // release: the entry is visible to the readers' acquire
+    st_shared_s32(q.entry(slot), u);
+    mbar_arrive(q.full(slot));  // release: the entry is visible to the readers' acquire
     ++n;
     return u;
   }
@@ -373,19 +400,19 @@ struct UnitReader {
   UnitRing q;
   unsigned* status;
   bool release;
-  long long n = 0;
+  int n = 0;
   bool lone = false;
   __device__ __forceinline__ int next() {
-    const int slot = (int)(n % UQ_DEPTH);
-    mbar_wait(q.full0 + 8 * slot, (unsigned)((n / UQ_DEPTH) & 1), status);
-    int u = q.slot[slot];
+    const int slot = n % UQ_DEPTH;
+    mbar_wait(q.full(slot), (unsigned)((n / UQ_DEPTH) & 1), status);
+    int u = ld_shared_s32(q.entry(slot));
     if ((*(volatile unsigned*)status & STATUS_WAIT_TIMEOUT) != 0u) u = -1;
     if (release) {
       if (lone) {
-        mbar_arrive(q.empty0 + 8 * slot);
+        mbar_arrive(q.empty(slot));
       } else {
         __syncwarp();
-        if ((threadIdx.x & 31) == 0) mbar_arrive(q.empty0 + 8 * slot);
+        if ((threadIdx.x & 31) == 0) mbar_arrive(q.empty(slot));
       }
     }
     ++n;
@@ -406,8 +433,8 @@ struct WarpClaimer {
 
 __device__ __forceinline__ void unit_ring_init(const UnitRing& q, unsigned readers) {
   for (int s = 0; s < UQ_DEPTH; ++s) {
-    mbar_init(q.full0 + 8 * s, 1);
-    mbar_init(q.empty0 + 8 * s, readers);
+    mbar_init(q.full(s), 1);
+    mbar_init(q.empty(s), readers);
   }
 }
 
@@ -470,7 +497,7 @@ struct JobBatch {
   __device__ __forceinline__ void acquire_maps(int j) const {
     const CUtensorMap* m = &jobs[j].tmA;
 #pragma unroll
-    for (int q = 0; q < 6; ++q)
+    for (int q = 0; q < 8; ++q)
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m + q) : "memory");
   }
 };
@@ -480,12 +507,12 @@ __device__ __forceinline__ void load_terms(const GemmArgs& a, LoadIter& it) {
   if (it.t < it.p.nb) it.tb = a.terms[it.p.b0 + it.t];
 }
 
-template <class Src>
+template <bool VARH = false, class Src>
 __device__ __forceinline__ void iter_enter_unit(const Src& src, LoadIter& it) {
   it.j = src.find(it.u);
   const GemmArgs& a = src.get(it.j);
   it.nks = (a.ks + BK - 1) / BK;
-  it.w = decode_unit(a, it.u - src.first_unit(it.j));
+  it.w = decode_unit<VARH>(a, it.u - src.first_unit(it.j));
   it.r = it.w.r0;
   it.p = a.prods[it.r];
   it.T = prod_T(it.p);
@@ -494,11 +521,11 @@ __device__ __forceinline__ void iter_enter_unit(const Src& src, LoadIter& it) {
   load_terms(a, it);
 }
 
-template <class Src, class Nx>
+template <bool VARH = false, class Src, class Nx>
 __device__ __forceinline__ void load_iter_start(const Src& src, LoadIter& it, Nx& nx) {
   it.u = nx.next();
   it.valid = it.u >= 0;
-  if (it.valid) iter_enter_unit(src, it);
+  if (it.valid) iter_enter_unit<VARH>(src, it);
 }
 
 template <class Src, class Nx>
@@ -700,7 +727,7 @@ __device__ __forceinline__ KStep kstep_info(const GemmArgs& a, const LoadIter& i
 }
 
 // Per-k-step iterator over (unit, product, k step); ta / tb hold the first A / B term.
-template <class Src, class Nx>
+template <bool VARH = false, class Src, class Nx>
 __device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it, Nx& nx) {
   it.t = 0;
   if (++it.s < it.nks) return;
@@ -717,7 +744,7 @@ __device__ __forceinline__ void kiter_next(const Src& src, LoadIter& it, Nx& nx)
     it.valid = false;
     return;
   }
-  iter_enter_unit(src, it);
+  iter_enter_unit<VARH>(src, it);
 }
 
 template <class Src>
@@ -899,7 +926,7 @@ __device__ __forceinline__ void frag_counts(int vr, int vc, int wm, int wn, int&
 // the whole 64 x 32 warp tile; fewer for the warps of an edge tile, whose other
 // fragments stay as they were and are never written out).  Compile-time counts keep each
 // form straight-line code: shared-memory loads and DMMAs with no predicates.
-template <int IM, int JN>
+template <int IM, int JN, int LDA = LDA_S>
 __device__ __forceinline__ void mma_stage_t(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
                                             int wn, int g, int t4) {
 #pragma unroll
@@ -908,8 +935,8 @@ __device__ __forceinline__ void mma_stage_t(const double* opA, const double* opB
 #pragma unroll
     for (int i = 0; i < IM; ++i) {
       const int row = wm * 64 + i * 16 + g;
-      af[i][0] = opA[(kq * 4 + t4) * LDA_S + row];
-      af[i][1] = opA[(kq * 4 + t4) * LDA_S + row + 8];
+      af[i][0] = opA[(kq * 4 + t4) * LDA + row];
+      af[i][1] = opA[(kq * 4 + t4) * LDA + row + 8];
     }
 #pragma unroll
     for (int j = 0; j < JN; ++j) bf[j] = opB[(frag_col(wn, j) + g) * LDB_S + kq * 4 + t4];
@@ -1104,9 +1131,7 @@ __device__ __forceinline__ void gemm_cta(const Src& src) {
   const unsigned empty0 = smem_u32(bars + NSTAGE);
   const unsigned rfull0 = smem_u32(bars + 2 * NSTAGE);
   const unsigned rempty0 = smem_u32(bars + 2 * NSTAGE + NRAW_TMA);
-  unsigned long long* rbars = bars + 2 * NSTAGE + 2 * NRAW_TMA;
-  const UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * UQ_DEPTH), smem_u32(rbars),
-                   smem_u32(rbars + UQ_DEPTH)};
+  const UnitRing q{smem_u32(bars + 2 * NSTAGE + 2 * NRAW_TMA)};
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
@@ -1184,7 +1209,7 @@ __device__ __forceinline__ void direct_issuer(const Src& src, double* stages, un
                                               const UnitRing& q) {
   UnitClaimer<Src> nx{src, q};
   LoadIter it;
-  load_iter_start(src, it, nx);
+  load_iter_start<true>(src, it, nx);
   long long kc = 0;
   int mapped = -1;
 #pragma unroll 1
@@ -1199,12 +1224,14 @@ __device__ __forceinline__ void direct_issuer(const Src& src, double* stages, un
     const int k0 = it.s * BK;
     mbar_wait(empty0 + 8 * stage, (unsigned)(((kc / NSTAGE_D) & 1) ^ 1), src.status());
     const unsigned fb = full0 + 8 * stage;
-    mbar_arrive_expect_tx(fb, TMA_BYTES_A + TMA_BYTES_B8);
-    tma_load_2d(smem_u32(opA), it.ta.src ? &a.tmAw : &a.tmA, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, fb);
+    const bool half = unit_half(a, it.w);  // half-height unit: a BM / 2-row A box, dense [k][BM / 2]
+    mbar_arrive_expect_tx(fb, (half ? TMA_BYTES_A / 2 : TMA_BYTES_A) + TMA_BYTES_B8);
+    const CUtensorMap* ma = it.ta.src ? (half ? &a.tmAw64 : &a.tmAw) : (half ? &a.tmA64 : &a.tmA);
+    tma_load_2d(smem_u32(opA), ma, it.ta.row * a.ms + it.w.m0, it.ta.col * a.ks + k0, fb);
     tma_load_2d(smem_u32(opA + OPA_SZ), it.tb.src ? &a.tmBw : &a.tmB, it.tb.row * a.ks + k0,
                 it.tb.col * a.ns + it.w.n0, fb);
     ++kc;
-    kiter_next(src, it, nx);
+    kiter_next<true>(src, it, nx);
   }
   // copies still in flight (only on an error path) land before the CTA exits
   for (long long q = kc - NSTAGE_D; q < kc; ++q)
@@ -1226,7 +1253,8 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
     const int job = src.find(u);
     const GemmArgs& a = src.get(job);
     const int nks = (a.ks + BK - 1) / BK;
-    const Unit w = decode_unit(a, u - src.first_unit(job));
+    const Unit w = decode_unit<true>(a, u - src.first_unit(job));
+    const bool half = unit_half(a, w);
     int im, jn;
     frag_counts(a.ms - w.m0, a.ns - w.n0, wm, wn, im, jn);
 #pragma unroll 1
@@ -1237,33 +1265,75 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
         for (int j = 0; j < 4; ++j)
 #pragma unroll
           for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
-      with_frags(im, jn, [&](auto fr) {
-        using FR = decltype(fr);
+      if (half) {
+        // both rows of warps on the tile's BM / 2 rows, warp row wm taking the k steps s with
+        // s % 2 == wm; every warp still waits for each stage before releasing it, so no
+        // release can land in the stage's previous phase
 #pragma unroll 1
         for (int s = 0; s < nks; ++s, ++kc) {
           const int stage = (int)(kc % NSTAGE_D);
           const double* opA = stages + (size_t)stage * STAGE_SZ;
           mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
-          mma_stage_t<FR::IM, FR::JN>(opA, opA + OPA_SZ, acc, wm, wn, g, t4);
-          __threadfence_block();  // fragment loads complete before the stage can be refilled
+          if ((s & 1) == wm) mma_stage_t<4, 4, BM / 2>(opA, opA + OPA_SZ, acc, 0, wn, g, t4);
+          __threadfence_block();
           __syncwarp();
           if (lane == 0) mbar_arrive(empty0 + 8 * stage);
         }
-      });
+      } else {
+        with_frags(im, jn, [&](auto fr) {
+          using FR = decltype(fr);
+#pragma unroll 1
+          for (int s = 0; s < nks; ++s, ++kc) {
+            const int stage = (int)(kc % NSTAGE_D);
+            const double* opA = stages + (size_t)stage * STAGE_SZ;
+            mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
+            mma_stage_t<FR::IM, FR::JN>(opA, opA + OPA_SZ, acc, wm, wn, g, t4);
+            __threadfence_block();  // fragment loads complete before the stage can be refilled
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty0 + 8 * stage);
+          }
+        });
+      }
       // hand the product tile to the epilogue warps once they are done with the previous one
       mbar_wait(mempty, (unsigned)((q & 1) ^ 1), src.status());
+      if (half) {  // rows 0..63: warp row 0's sums, then warp row 1's added
+        if (wm == 0) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < 4; ++j)
 #pragma unroll
-          for (int h = 0; h < 2; ++h)
+              for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int rr = wm * 64 + i * 16 + g + 8 * h;
-              const int cc = frag_col(wn, j) + t4 * 2 + e;
-              Ms[cc * MS_LD + rr] = acc[i][j][2 * h + e];
-            }
+                for (int e = 0; e < 2; ++e)
+                  Ms[(frag_col(wn, j) + t4 * 2 + e) * MS_LD + i * 16 + g + 8 * h] = acc[i][j][2 * h + e];
+        }
+        named_bar_sync(3, NCONS);
+        if (wm == 1) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+              for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                  Ms[(frag_col(wn, j) + t4 * 2 + e) * MS_LD + i * 16 + g + 8 * h] += acc[i][j][2 * h + e];
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int rr = wm * 64 + i * 16 + g + 8 * h;
+                const int cc = frag_col(wn, j) + t4 * 2 + e;
+                Ms[cc * MS_LD + rr] = acc[i][j][2 * h + e];
+              }
+      }
       __syncwarp();
       if (lane == 0) mbar_arrive(mfull);
     }
@@ -1284,7 +1354,8 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
     const int ul = u - src.first_unit(job);
     const int ntiles = a.tiles_m * a.tiles_n;
     const bool ordered = (a.mode == MODE_ACCUM_C) && a.chunks > 1;
-    const Unit w = decode_unit(a, ul);
+    const Unit w = decode_unit<true>(a, ul);
+    const int rows = unit_rows(a, w);
     const int chunk = ul / ntiles;
 #pragma unroll 1
     for (int r = w.r0; r < w.r1; ++r, ++q) {
@@ -1294,14 +1365,15 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
         const Term tm = a.terms[p.c0 + c];
         const double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc;
         for (int l = et; l < (BM / 16) * BN; l += NEPI_D) {
-          const int rr = w.m0 + (l % (BM / 16)) * 16, cc = w.n0 + l / (BM / 16);
-          if (rr < a.ms && cc < a.ns) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Cb + rr + (long long)cc * a.ldc));
+          const int ri = (l % (BM / 16)) * 16, cc = w.n0 + l / (BM / 16);
+          if (ri < rows && cc < a.ns)
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(Cb + w.m0 + ri + (long long)cc * a.ldc));
         }
       }
       mbar_wait(mfull, (unsigned)(q & 1), src.status());
       if (a.mode == MODE_STORE_M) {  // the product tile to its workspace (the AB pack type)
         double* Mr = a.M + (long long)r * a.m_stride + w.m0 + lane;
-        const int rmax = a.ms - w.m0 - lane;
+        const int rmax = rows - lane;
 #pragma unroll 1
         for (int col = ew; col < BN; col += NW) {
           if (w.n0 + col >= a.ns) continue;
@@ -1333,7 +1405,7 @@ __device__ __forceinline__ void direct_epilogue(const Src& src, const double* Ms
           named_bar_sync(2, NEPI_D);
         }
         double* Cb = a.C + (long long)tm.row * a.ms + (long long)tm.col * a.ns * a.ldc + w.m0 + lane;
-        const int rmax = a.ms - w.m0 - lane;  // rows of this lane inside the block: rr < rmax
+        const int rmax = rows - lane;  // rows of this lane inside the tile: rr < rmax
 #pragma unroll 1
         for (int col0 = ew; col0 < BN; col0 += NW * 4) {
           double cv[4][4];
@@ -1383,9 +1455,7 @@ __device__ __forceinline__ void gemm_cta_direct(const Src& src) {
   const unsigned empty0 = smem_u32(bars + NSTAGE_D);
   const unsigned mfull = smem_u32(bars + 2 * NSTAGE_D);
   const unsigned mempty = smem_u32(bars + 2 * NSTAGE_D + 1);
-  unsigned long long* rbars = bars + 2 * NSTAGE_D + 2;
-  const UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * UQ_DEPTH), smem_u32(rbars),
-                   smem_u32(rbars + UQ_DEPTH)};
+  const UnitRing q{smem_u32(bars + 2 * NSTAGE_D + 2)};
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE_D; ++s) {

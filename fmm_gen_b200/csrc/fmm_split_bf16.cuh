@@ -194,9 +194,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) fmm_split_gemm_kernel(const __gri
   const unsigned acce0 = fmm::smem_u32(bars + 2 * NSTG + NACC);  // [NACC] chunk drained
   const unsigned done_bar = fmm::smem_u32(bars + 2 * NSTG + 2 * NACC);  // every MMA complete
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + NBARS);
-  unsigned long long* rbars = bars + NBARS + 2;
-  const fmm::UnitRing q{reinterpret_cast<volatile int*>(rbars + 2 * fmm::UQ_DEPTH), fmm::smem_u32(rbars),
-                        fmm::smem_u32(rbars + fmm::UQ_DEPTH)};
+  const fmm::UnitRing q{fmm::smem_u32(bars + NBARS + 2)};
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nks = a.kpad / BK;
 

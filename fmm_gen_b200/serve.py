@@ -152,6 +152,8 @@ class Report:
     by_kind: Dict[str, Dict[str, float]] = field(default_factory=dict)
     launches: Dict[str, int] = field(default_factory=dict)
     peak_bytes: int = 0
+    run_s: float = 0.0            # the loop's duration (window plus the drain of admitted work)
+    stream_busy_s: Dict[str, float] = field(default_factory=dict)  # per stream: device time of its launches
 
     def percentile(self, q: float) -> Optional[float]:
         return float(np.percentile(self.latencies, q)) if self.latencies else None
@@ -164,6 +166,9 @@ class Report:
             "p99_ms": None if not self.latencies else 1e3 * self.percentile(99),
             "tflops_effective": self.flops_done / self.window / 1e12,
             "by_kind": self.by_kind, "launches": self.launches, "peak_admitted_gb": self.peak_bytes / 1e9,
+            "run_s": self.run_s,
+            "stream_busy_s": self.stream_busy_s,
+            "stream_busy_frac": {k: v / self.run_s for k, v in self.stream_busy_s.items()} if self.run_s else {},
         }
 
 
@@ -246,18 +251,21 @@ class Server:
             else:
                 self.sleep(2e-5)
         self.ex.sync()
+        run_s = self.clock() - t0
         arrived = [r for r in reqs if r.arrival < window]
         done_in = [r for r in arrived if r.done is not None and r.done <= window]
         rep = Report(window=window, offered=len(arrived), completed=len(done_in), rejected=rejected,
                      backlog=sum(1 for r in arrived if r.done is None or r.done > window) - rejected,
                      latencies=[r.latency for r in done_in], flops_done=sum(r.flops for r in done_in),
-                     launches=launches, peak_bytes=peak)
+                     launches=launches, peak_bytes=peak, run_s=run_s,
+                     stream_busy_s=self.ex.busy_seconds() if hasattr(self.ex, "busy_seconds") else {})
         for kind in (FP64, SPLIT):
             ks = [r for r in done_in if r.kind == kind]
             if ks:
                 lat = [r.latency for r in ks]
                 rep.by_kind[kind] = {"completed": len(ks), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
                                      "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                                     "flops_done": sum(r.flops for r in ks),
                                      "tflops_effective": sum(r.flops for r in ks) / window / 1e12}
         return rep
 
@@ -278,6 +286,7 @@ class GpuExecutor:
         self.streams = {FP64: torch.cuda.Stream(), SPLIT: torch.cuda.Stream()}
         self.plans: Dict[str, object] = {}
         self.results: Dict[int, object] = {}
+        self.marks: Dict[str, list] = {FP64: [], SPLIT: []}  # (start, end) timing events per launch
 
     def plan(self, name: str):
         if name == "classical":
@@ -310,15 +319,23 @@ class GpuExecutor:
         torch, rt = self.torch, self.rt
         st = self.streams[kind]
         with torch.cuda.stream(st):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
             if kind == FP64:
                 rt.batch_submit([self.plan(r.algorithm) for r in reqs], [r.handle[0] for r in reqs],
                                 [r.handle[1] for r in reqs], [r.handle[2] for r in reqs], stream=st)
             else:
                 for r in reqs:
                     rt.split_gemm(self.plan(r.algorithm), *r.handle, stream=st)
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(st)
+        self.marks[kind].append((e0, ev))
         return ev
+
+    def busy_seconds(self) -> Dict[str, float]:
+        """Device time each stream spent in its launches (after sync()): a launch's events
+        bracket its work on its stream, and launches of one stream run one after another."""
+        return {k: sum(a.elapsed_time(b) for a, b in v) / 1e3 for k, v in self.marks.items() if v}
 
     def done(self, token) -> bool:
         return token.query()

@@ -336,3 +336,34 @@ def test_gpu_ksplit_matches_oracle(oracle_lib, algo, shape):
     torch.cuda.synchronize()
     assert rt.load_library().fmm_device_status(1) == 0
     assert rel_fro(dC.cpu().numpy(), want) <= RTOL_SMALL
+
+
+# The last tile row of a block with at most 64 rows runs as a half-height unit in the direct
+# variant (a 64-row A box; both rows of consumer warps on those rows, alternate k steps):
+# plain 1050 x 700 x 512 (26-row edge), plain 64 x 300 x 256 (one 64-row tile row), 222-1 at
+# 2100 x 1800 x 1200 (pre-summed, ms = 1048: 24-row edge), 222-1 x 333-1 at 3312 x 2000 x 960
+# (pre-summed, ms = 552: 40-row edge, as at 16384^3).
+HALF_CASES = [
+    (None, (1050, 700, 512)),
+    (None, (64, 300, 256)),
+    ((["222"], [1]), (2100, 1800, 1200)),
+    ((["222", "333"], [1, 1]), (3312, 2000, 960)),
+]
+
+
+@pytest.mark.parametrize("algo,shape", HALF_CASES, ids=lambda x: str(x))
+def test_gpu_half_height_edge_tiles(oracle_lib, algo, shape):
+    m, n, k = shape
+    A, B, C = inputs(3 * m + n + k, m, n, k)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    want = C.copy(order="F")
+    if algo is None:
+        rt.plain_gemm(dA, dB, dC)
+        oracle_lib.bl_dgemm(A, B, want)
+    else:
+        p = plan_for(*algo)
+        rt.fmm_gemm(p, dA, dB, dC, "abc")
+        oracle_lib.fmm(tables(p.algebra), "abc", A, B, want)
+    torch.cuda.synchronize()
+    assert rt.load_library().fmm_device_status(1) == 0
+    assert rel_fro(dC.cpu().numpy(), want) <= RTOL_SMALL
