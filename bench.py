@@ -506,12 +506,14 @@ def main():
     peak = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
     del a, b, c
 
-    # ---- correctness of this run's result against a classical FP64 GEMM ----
-    errs = {}
+    # ---- correctness of this run's result against a classical FP64 GEMM; workspace per call ----
+    errs, ws_bytes = {}, {}
     for (m, n, k), (A, B, C) in zip(SHAPES, mats):
         C0 = rt.colmajor(m, n, device=dev).copy_(C)
         ref = torch.addmm(C0, A, B)
         rt.fmm_gemm(plan, A, B, C0, PACK)
+        torch.cuda.synchronize()
+        ws_bytes[f"{m}x{n}x{k}"] = rt.last_workspace_bytes()
         errs[f"{m}x{n}x{k}"] = ((C0 - ref).norm() / ref.norm()).item()
         del C0, ref
     torch.cuda.empty_cache()
@@ -534,8 +536,16 @@ def main():
     A16, B16, C16 = mats[0]
     p1 = rt.Plan.from_levels(["222"], [1])
     s222 = time_call(lambda: rt.fmm_gemm(p1, A16, B16, C16, "abc"))
+    ws222 = rt.last_workspace_bytes()
     s_plain16 = time_call(lambda: rt.plain_gemm(A16, B16, C16))
     f16 = 2.0 * 16384 ** 3
+    # the per-shape rate of the workload's algorithm beside the plain kernel
+    per_shape = {}
+    for (m, n, k), (A, B, C) in zip(SHAPES, mats):
+        tf = time_call(lambda A=A, B=B, C=C: rt.fmm_gemm(plan, A, B, C, PACK))
+        tp = time_call(lambda A=A, B=B, C=C: rt.plain_gemm(A, B, C))
+        per_shape[f"{m}x{n}x{k}"] = {"fmm_tflops": 2.0 * m * n * k / (tf * 1e-3) / 1e12,
+                                     "plain_tflops": 2.0 * m * n * k / (tp * 1e-3) / 1e12, "ratio": tp / tf}
 
     # ---- end to end through the host C ABI (pinned host buffers, copies in the timed region) ----
     host = []
@@ -611,7 +621,10 @@ def main():
             "plain_fp64": {"tflops": plain_tflops, "fmm_over_plain": value / world / plain_tflops},
             "strassen_222_1_16384": {"fmm_tflops": f16 / (s222 * 1e-3) / 1e12,
                                      "plain_tflops": f16 / (s_plain16 * 1e-3) / 1e12,
-                                     "ratio": s_plain16 / s222},
+                                     "ratio": s_plain16 / s222, "workspace_bytes": ws222},
+            "per_shape": per_shape,
+            "workspace": {"limit_bytes": rt.set_workspace_limit(0), "per_call_bytes": ws_bytes,
+                          "note": "pre-summed operand workspace; calls above the limit run their products in groups"},
             "rel_fro_err_vs_cublas": errs,
         }
         line.update(extra)

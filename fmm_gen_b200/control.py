@@ -27,7 +27,7 @@ import os
 import shutil
 import subprocess
 import sys
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 from . import algebra
 from .alg_dic import alg_dic
@@ -167,13 +167,15 @@ def _cc() -> str:
 
 
 def generate_code(algs: Sequence[str], levels: Sequence[int], pack_type: str = "abc", path_prefix: str = "../",
-                  compile_code: bool = True) -> str:
-    """Write (and by default compile) the job directory; returns its path."""
+                  compile_code: bool = True, x: Optional[float] = None) -> str:
+    """Write (and by default compile) the job directory; returns its path.  `x` is the value
+    of the approximate algorithms' parameter (the reference leaves it symbolic in its generated
+    C, meta/common_util.py:56-60); it must be given when a level uses one."""
     job = job_name(algs, levels, pack_type)
     d = os.path.join(os.path.abspath(path_prefix), job)
     for sub in ("dgemm", "lib", "test", "include"):
         os.makedirs(os.path.join(d, sub), exist_ok=True)
-    plan = algebra.make_plan(list(algs), list(levels))
+    plan = algebra.make_plan(list(algs), list(levels), x=x)
     with open(os.path.join(d, "plan.json"), "w") as fh:
         json.dump({"job": job, "levels": [[a, int(l)] for a, l in zip(algs, levels)], "dims": list(plan.dims),
                    "rank": plan.rank, "pack_type": pack_type,
@@ -205,11 +207,19 @@ def generate_code(algs: Sequence[str], levels: Sequence[int], pack_type: str = "
 
 def main(argv=None) -> None:
     argv = list(sys.argv[1:] if argv is None else argv)
+    x = None
+    if "--x" in argv:  # value of the approximate algorithms' parameter (an addition to the CLI)
+        i = argv.index("--x")
+        try:
+            x = float(argv[i + 1])
+        except (IndexError, ValueError):
+            raise SystemExit("--x needs a number")
+        del argv[i:i + 2]
     algs, levels, pack_type, gen_path = parse_argv(argv)
     from .build import build
 
     build()
-    d = generate_code(algs, levels, pack_type, gen_path)
+    d = generate_code(algs, levels, pack_type, gen_path, x=x)
     print(d)
 
 

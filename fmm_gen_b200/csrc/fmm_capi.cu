@@ -36,6 +36,11 @@ std::atomic<long long> g_launches{0};
 thread_local int t_last_error = FMM_OK;
 // Byte written into every ticket before a launch (fmm_debug_set): 0 in normal operation.
 int g_ticket_fill = 0;
+// Cap on the pre-summed operand workspace of one call (fmm_set_workspace_limit), and the
+// workspace bytes the last call on this thread used.
+constexpr long long kDefaultWorkspaceLimit = 4LL << 30;
+std::atomic<long long> g_ws_limit{kDefaultWorkspaceLimit};
+thread_local long long t_last_ws = 0;
 
 // Optional per-kernel timing: when enabled, every launch is bracketed by CUDA events on
 // its own stream; fmm_profile_end() sums the durations per kernel kind.
@@ -108,9 +113,9 @@ struct DevTables {
 
 // Tables of a k split (see ksplit_tables): base tables (one of the TableBase forms) with
 // every product r split into S products (r, p) over k range p of its operands.
-enum TableBase : int { BASE_ORIG = 0, BASE_PS = 1, BASE_ALL = 2 };
+enum TableBase : int { BASE_ORIG = 0, BASE_PS = 1, BASE_ALL = 2, BASE_GROUP = 3 };
 struct KSplitTables {
-  int base = 0, S = 0, dev = -1;
+  int base = 0, S = 0, g1 = 0, dev = -1;  // BASE_GROUP: products [S, g1) (see group_build)
   fmm::Prod* prods = nullptr;
   fmm::Term* terms = nullptr;
 };
@@ -255,24 +260,55 @@ void ksplit_build(const fmm_plan* p, int base, int S, std::vector<fmm::Prod>* op
   }
 }
 
-// The k-split tables of a plan on the current device (uploaded on first use).
-int ksplit_tables(const fmm_plan* cp, int base, int S, const fmm::Prod** prods, const fmm::Term** terms) {
+// Tables of products [g0, g1) over the slots of a group workspace: product r reads slot
+// r - g0 of S and of T (src 1), keeps its C terms, and counts its per-block ticket positions
+// within the group (each group is a launch of its own).
+void group_build(const fmm_plan* p, int g0, int g1, std::vector<fmm::Prod>* op, std::vector<fmm::Term>* ot) {
+  std::vector<int> cnt((size_t)p->dims[0] * p->dims[2], 0);
+  for (int r = g0; r < g1; ++r) {
+    const fmm::Prod& pr = p->prods[r];
+    fmm::Prod v{};
+    v.a0 = (int)ot->size();
+    v.na = 1;
+    ot->push_back(fmm::Term{0, r - g0, 1.0, 1, 0});
+    v.b0 = (int)ot->size();
+    v.nb = 1;
+    ot->push_back(fmm::Term{0, r - g0, 1.0, 1, 0});
+    v.c0 = (int)ot->size();
+    v.nc = pr.nc;
+    for (int t = 0; t < pr.nc; ++t) {
+      fmm::Term x = p->terms[pr.c0 + t];
+      x.pad = cnt[(size_t)x.row * p->dims[2] + x.col]++;
+      ot->push_back(x);
+    }
+    op->push_back(v);
+  }
+}
+
+// Derived tables of a plan on the current device (uploaded on first use): the k split S of a
+// base form (ksplit_build), or with base == BASE_GROUP the group [S, g1) (group_build).
+int ksplit_tables(const fmm_plan* cp, int base, int S, const fmm::Prod** prods, const fmm::Term** terms,
+                  int g1 = 0) {
   fmm_plan* p = const_cast<fmm_plan*>(cp);
   int dev = 0;
   FMM_CUDA_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(p->mu);
   for (const auto& t : p->ksplit)
-    if (t.base == base && t.S == S && t.dev == dev) {
+    if (t.base == base && t.S == S && t.g1 == g1 && t.dev == dev) {
       *prods = t.prods;
       *terms = t.terms;
       return FMM_OK;
     }
   std::vector<fmm::Prod> vp;
   std::vector<fmm::Term> vt;
-  ksplit_build(p, base, S, &vp, &vt);
+  if (base == BASE_GROUP)
+    group_build(p, S, g1, &vp, &vt);
+  else
+    ksplit_build(p, base, S, &vp, &vt);
   KSplitTables t;
   t.base = base;
   t.S = S;
+  t.g1 = g1;
   t.dev = dev;
   FMM_CUDA_TRY(cudaMalloc(&t.prods, sizeof(fmm::Prod) * vp.size()));
   cudaError_t e = cudaMalloc(&t.terms, sizeof(fmm::Term) * vt.size());
@@ -889,6 +925,92 @@ int presum_prepare(const fmm_plan* plan, const DevTables& d, const double* A, lo
   return rc;
 }
 
+// Bytes presum_prepare would allocate for one call.
+size_t presum_bytes(const fmm_plan* plan, int ms, int ns, int ks) {
+  if (ks % fmm::BK != 0) {
+    const size_t kp = (ks + fmm::BK - 1) / fmm::BK * fmm::BK;
+    return sizeof(double) * kp * ((size_t)ms + ns) * plan->rank + 16;
+  }
+  return sizeof(double) * ((size_t)ms * ks * plan->plistA.size() + (size_t)(ks + (ks & 1)) * ns * plan->plistB.size()) +
+         16;
+}
+
+// Pre-summed products in groups, when one call's whole operand workspace would exceed the
+// workspace limit: the R products run as groups of G consecutive products, each group's
+// operand sums (one slot per product, k extent padded to whole k steps) formed into one of
+// two workspace halves while the previous group's products run.  The sums go on a second
+// stream, which waits for the products that last read that half; each group's products
+// wait for their sums.  Groups run in product order on the caller's stream, so every C
+// element still receives its products' updates in order r = 0..R-1 (results are those of
+// the ungrouped call).  Workspace 2 G (ms + ns) kk 8 bytes, within the limit for G >= 1.
+int run_presum_groups(const fmm_plan* plan, const DevTables& d, const double* A, long long lda, const double* B,
+                      long long ldb, double* C, long long ldc, int ms, int ns, int ks, cudaStream_t st) {
+  const int R = plan->rank;
+  const int kk = (ks + fmm::BK - 1) / fmm::BK * fmm::BK;
+  const size_t sb = sizeof(double) * (size_t)ms * kk, tb = sizeof(double) * (size_t)kk * ns;
+  long long G = g_ws_limit.load() / (long long)(2 * (sb + tb));
+  G = std::max<long long>(1, std::min<long long>(G, R));
+  const int ng = (int)((R + G - 1) / G);
+  const int nbuf = ng > 1 ? 2 : 1;
+  const size_t half = (size_t)G * (sb + tb);
+  char* ws = nullptr;
+  FMM_CUDA_TRY(cudaMallocAsync((void**)&ws, nbuf * half + 16, st));
+  t_last_ws = (long long)(nbuf * half);
+  int rc = FMM_OK;
+  auto ok = [&](cudaError_t e) {
+    if (rc == FMM_OK && e != cudaSuccess) rc = cuda_status(e);
+    return rc == FMM_OK;
+  };
+  // zero padding once per half: S slot columns [ks, kk), T slot rows [ks, kk) (the sums fill [0, ks))
+  for (int b = 0; b < nbuf && kk != ks; ++b) {
+    char* S = ws + b * half;
+    ok(cudaMemset2DAsync(S + sizeof(double) * (size_t)ms * ks, sb, 0, sizeof(double) * (size_t)ms * (kk - ks), G,
+                         st)) &&
+        ok(cudaMemset2DAsync(S + G * sb + sizeof(double) * ks, sizeof(double) * kk, 0, sizeof(double) * (kk - ks),
+                             (size_t)G * ns, st));
+  }
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_sum[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
+  ok(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) &&
+      ok(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming)) &&
+      ok(cudaEventCreateWithFlags(&ev_sum[0], cudaEventDisableTiming)) &&
+      ok(cudaEventCreateWithFlags(&ev_sum[1], cudaEventDisableTiming)) &&
+      ok(cudaEventCreateWithFlags(&ev_done[0], cudaEventDisableTiming)) &&
+      ok(cudaEventCreateWithFlags(&ev_done[1], cudaEventDisableTiming)) && ok(cudaEventRecord(ev_start, st)) &&
+      ok(cudaStreamWaitEvent(side, ev_start, 0));
+  for (int g = 0; g < ng && rc == FMM_OK; ++g) {
+    const int g0 = (int)(g * G), g1 = (int)std::min<long long>(R, (g + 1) * G), n = g1 - g0, b = g % 2;
+    char* S = ws + b * half;
+    PresumOps ps;
+    ps.plistA = d.plist_all + g0;
+    ps.plistB = d.plist_all + g0;
+    ps.kslot = kk;
+    ps.S = reinterpret_cast<const double*>(S);
+    ps.ldS = ms;
+    ps.nslotA = n;
+    ps.T = reinterpret_cast<const double*>(S + G * sb);
+    ps.ldT = kk;
+    ps.nslotB = n;
+    if (g >= 2 && !ok(cudaStreamWaitEvent(side, ev_done[b], 0))) break;
+    rc = presum(d, A, lda, B, ldb, ps, ms, ns, ks, side);
+    if (!ok(cudaEventRecord(ev_sum[b], side)) || !ok(cudaStreamWaitEvent(st, ev_sum[b], 0))) break;
+    const fmm::Prod* gp = nullptr;
+    const fmm::Term* gt = nullptr;
+    if (rc == FMM_OK) rc = ksplit_tables(plan, BASE_GROUP, g0, &gp, &gt, g1);
+    if (rc == FMM_OK)
+      rc = launch_gemm(K_GEMM_FMM, gp, gt, plan->dims, n, fmm::MODE_ACCUM_C, A, lda, B, ldb, ps, C, ldc, nullptr, 0,
+                       0, ms, ns, kk, st, true, ks);
+    if (rc == FMM_OK) ok(cudaEventRecord(ev_done[b], st));
+  }
+  // every sum was waited for by the caller's stream, so freeing there comes after all uses
+  cudaError_t fe = cudaFreeAsync(ws, st);
+  if (rc == FMM_OK) rc = cuda_status(fe);
+  for (cudaEvent_t e : {ev_start, ev_sum[0], ev_sum[1], ev_done[0], ev_done[1]})
+    if (e) cudaEventDestroy(e);
+  if (side) cudaStreamDestroy(side);
+  return rc;
+}
+
 int check_args(int m, int n, int k, const void* A, long long lda, const void* B, long long ldb, const void* C,
                long long ldc) {
   if (m < 0 || n < 0 || k < 0) return FMM_E_INVALID;
@@ -912,6 +1034,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
   rc = device_tables(plan, &d);
   if (rc != FMM_OK) return rc;
   const int R = plan->rank;
+  t_last_ws = 0;
   if (ms > 0 && ns > 0 && ks > 0) {
     if (pack == FMM_PACK_ABC) {
       const int nA = (int)plan->plistA.size(), nB = (int)plan->plistB.size();
@@ -934,9 +1057,12 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         }
         cudaError_t fe = cudaFreeAsync(mws, st);
         if (rc == FMM_OK) rc = cuda_status(fe);
+      } else if (use_presum(plan, ms, ns, ks) && (long long)presum_bytes(plan, ms, ns, ks) > g_ws_limit.load()) {
+        rc = run_presum_groups(plan, *d, A, lda, B, ldb, C, ldc, ms, ns, ks, st);  // workspace within the limit
       } else if (use_presum(plan, ms, ns, ks)) {
         // U/V sums formed once per product in HBM (bandwidth-bound), then every
         // product reads single operands; products scattered into C in the epilogue.
+        t_last_ws = (long long)presum_bytes(plan, ms, ns, ks);
         PresumPlan pp;
         rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
         const long long units = (long long)((ms + fmm::BM - 1) / fmm::BM) * ((ns + fmm::BN - 1) / fmm::BN) * R;
@@ -1383,6 +1509,12 @@ const char* fmm_error_string(int code) {
 long long fmm_kernel_launch_count(void) { return g_launches.load(); }
 
 int fmm_device_status(int clear) { return device_status(clear != 0); }
+
+long long fmm_set_workspace_limit(long long bytes) {
+  return g_ws_limit.exchange(bytes > 0 ? bytes : kDefaultWorkspaceLimit);
+}
+
+long long fmm_last_workspace_bytes(void) { return t_last_ws; }
 
 int fmm_debug_set(int what, long long value) {
   switch (what) {

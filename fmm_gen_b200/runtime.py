@@ -125,6 +125,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_device_status.restype = c_int
     lib.fmm_debug_set.argtypes = [c_int, ctypes.c_longlong]
     lib.fmm_debug_set.restype = c_int
+    lib.fmm_set_workspace_limit.argtypes = [ctypes.c_longlong]
+    lib.fmm_set_workspace_limit.restype = ctypes.c_longlong
+    lib.fmm_last_workspace_bytes.argtypes = []
+    lib.fmm_last_workspace_bytes.restype = ctypes.c_longlong
 
 
 def _check(rc: int, what: str) -> None:
@@ -165,8 +169,10 @@ class Plan:
         self.handle = h
 
     @classmethod
-    def from_levels(cls, algs, levels) -> "Plan":
-        return cls(algebra.make_plan(algs, levels))
+    def from_levels(cls, algs, levels, x: Optional[float] = None) -> "Plan":
+        """The composed plan of e.g. (['222', '333'], [1, 1]); `x` is the value of the
+        approximate algorithms' parameter (alg_dic's *_approx entries)."""
+        return cls(algebra.make_plan(algs, levels, x=x))
 
     @property
     def rank(self) -> int:
@@ -377,6 +383,17 @@ def bl_dgemm_host(A: np.ndarray, B: np.ndarray, C: np.ndarray) -> None:
     n = B.shape[1]
     lib.bl_dgemm(m, n, k, A.ctypes.data, _np_ld(A), B.ctypes.data, _np_ld(B), C.ctypes.data, _np_ld(C))
     _check(lib.fmm_last_error(), "bl_dgemm")
+
+
+def set_workspace_limit(nbytes: int) -> int:
+    """Cap one call's pre-summed operand workspace (bytes <= 0: the default, 4 GiB); returns
+    the previous cap.  Calls that would need more run their products in groups."""
+    return int(load_library().fmm_set_workspace_limit(int(nbytes)))
+
+
+def last_workspace_bytes() -> int:
+    """Pre-summed workspace bytes of this thread's last FMM call."""
+    return int(load_library().fmm_last_workspace_bytes())
 
 
 def kernel_launch_count() -> int:

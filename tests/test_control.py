@@ -58,3 +58,19 @@ def test_job_library_binds_its_plan_on_load(tmp_path):
     assert job.fmm_job_status() == 0
     h = L.fmm_default_plan()
     assert h and L.fmm_plan_rank(h) == 11
+
+
+def test_generator_accepts_the_approximate_parameter(tmp_path):
+    """An approximate algorithm's job needs a value for x (--x on the CLI); the job's
+    plan.json then holds the evaluated coefficients."""
+    import json
+
+    from fmm_gen_b200 import algebra, control
+
+    d = control.generate_code(["bini322_10_52_approx"], [1], "abc", str(tmp_path), compile_code=False, x=0.25)
+    with open(os.path.join(d, "plan.json")) as fh:
+        plan = json.load(fh)
+    want = algebra.make_plan(["bini322_10_52_approx"], [1], x=0.25)
+    assert plan["rank"] == want.rank == 10
+    coefs = [abs(c[2]) for p in plan["products"] for side in ("a", "b", "c") for c in p[side]]
+    assert max(coefs) == 4.0 == float(abs(want.W).max())  # 1 / x

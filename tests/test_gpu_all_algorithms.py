@@ -69,3 +69,23 @@ def test_every_partition_split_bf16(oracle_lib, name):
 def test_two_level_plans(oracle_lib, algs, levels):
     assert run_case(oracle_lib, algs, levels, split=False) <= RTOL_FP64
     assert run_case(oracle_lib, algs, levels, split=True) <= RTOL_SPLIT
+
+
+# Approximate (APA) algorithms: the coefficient files use a parameter x (the reference keeps it
+# symbolic in its generated C, meta/common_util.py:56-60); Plan.from_levels takes its value.
+@pytest.mark.parametrize("name", ["bini322_10_52_approx", "smirnov323_14_108_approx"])
+def test_gpu_approximate_algorithm_matches_oracle(oracle_lib, name):
+    p = rt.Plan.from_levels([name], [1], x=0.5)
+    m, n, k = shape_for(p.algebra.dims)
+    rng = np.random.default_rng(len(name) + m)
+    A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    dA = rt.colmajor(m, k, device="cuda").copy_(torch.from_numpy(A))
+    dB = rt.colmajor(k, n, device="cuda").copy_(torch.from_numpy(B))
+    dC = rt.colmajor(m, n, device="cuda").copy_(torch.from_numpy(C))
+    rt.fmm_gemm(p, dA, dB, dC, "abc")
+    want = C.copy(order="F")
+    dims, nterms, rows, cols, coefs = rt.plan_tables(p.algebra)
+    oracle_lib.fmm((dims, p.rank, nterms, rows, cols, coefs), "abc", A, B, want)
+    assert float(np.linalg.norm(dC.cpu().numpy() - want) / np.linalg.norm(want)) <= RTOL_FP64

@@ -367,3 +367,37 @@ def test_gpu_half_height_edge_tiles(oracle_lib, algo, shape):
     torch.cuda.synchronize()
     assert rt.load_library().fmm_device_status(1) == 0
     assert rel_fro(dC.cpu().numpy(), want) <= RTOL_SMALL
+
+
+# A call whose pre-summed workspace would exceed the workspace limit runs its products in
+# groups (sums of the next group formed on a second stream while a group runs).  Small
+# limits force 2..7 groups here; results match the oracle and the ungrouped call.
+@pytest.mark.parametrize("algs,levels,shape,limit", [
+    (["222"], [1], (2048, 2048, 1024), 16 << 20),         # one product per group (2 x 8 MB)
+    (["222"], [1], (2048, 2048, 1024), 32 << 20),         # groups of 2 (last group smaller)
+    (["222", "333"], [1, 1], (2000, 2000, 1000), 40 << 20),  # k per product 166: padded slots
+])
+def test_gpu_presum_groups_match_oracle(oracle_lib, algs, levels, shape, limit):
+    m, n, k = shape
+    A, B, C = inputs(m + n + k + limit % 997, m, n, k)
+    p = plan_for(algs, levels)
+    dA, dB = to_dev(A), to_dev(B)
+    whole = to_dev(C)
+    rt.fmm_gemm(p, dA, dB, whole, "abc")
+    torch.cuda.synchronize()
+    full = rt.last_workspace_bytes()
+    assert full > limit
+    prev = rt.set_workspace_limit(limit)
+    try:
+        dC = to_dev(C)
+        rt.fmm_gemm(p, dA, dB, dC, "abc")
+        torch.cuda.synchronize()
+        assert 0 < rt.last_workspace_bytes() <= limit
+    finally:
+        rt.set_workspace_limit(prev)
+    assert rt.load_library().fmm_device_status(1) == 0
+    want = C.copy(order="F")
+    oracle_lib.fmm(tables(p.algebra), "abc", A, B, want)
+    got = dC.cpu().numpy()
+    assert rel_fro(got, want) <= RTOL_SMALL
+    assert rel_fro(got, whole.cpu().numpy()) <= RTOL_SMALL
