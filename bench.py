@@ -343,7 +343,7 @@ def batch_512(rt, torch, dev, steps=3):
     for c in set(rep.choices) - {"classical"} - set(measure.plans):
         measure.plans[c] = rt.Plan.from_levels(*tuner.candidate_levels(c))
     plans = [None if c == "classical" else measure.plans[c] for c in rep.choices]
-    batch = rt.Batch(shapes, plans)
+    batch = rt.Batch(shapes, plans, tiles=rep.tiles)
     s = torch.cuda.Stream(device=dev)
     s.wait_stream(torch.cuda.current_stream(dev))
     with torch.cuda.stream(s):
@@ -369,7 +369,8 @@ def batch_512(rt, torch, dev, steps=3):
     out = {"problems": len(shapes), "dims": "log-uniform [256, 4096], seed 0", "total_flop": flops,
            "ms": ms, "tflops_effective": flops / (ms * 1e-3) / 1e12,
            "all_classical_ms": classical_ms, "model_ms": model_ms,
-           "choices": rep.counts(), "tune_s": tune_s, "tune_trials": rep.trials,
+           "choices": rep.counts(), "choices_key": "algorithm/tile rows", "tune_s": tune_s,
+           "tune_trials": rep.trials,
            "launches_per_replay": launches_per_replay}
     del As, Bs, Cs
     torch.cuda.empty_cache()

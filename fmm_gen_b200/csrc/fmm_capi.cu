@@ -1979,6 +1979,7 @@ struct fmm_batch {
     size_t ws_off;                 // byte offset of S (then T) in the workspace
     long long ldT;
     int chunks, tiles_m, tiles_n, units;
+    int bm;                        // tile height: fmm::BM, or BM / 2 (direct phases only)
     size_t ticket_off;             // int offset into the ticket array
     double cost;                   // estimated k steps per unit (scheduling order)
   };
@@ -2042,10 +2043,11 @@ int batch_chunks(int nprod, int ks) {
 }
 
 void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int ms, int ns, int ks, int a_r, int a_c,
-                   int b_r, int b_c, int c_r, int c_c) {
+                   int b_r, int b_c, int c_r, int c_c, int bm) {
   if (ms <= 0 || ns <= 0 || ks <= 0) return;
   fmm_batch::Job j{};
   j.prob = prob;
+  j.bm = bm;
   j.plan = plan;
   std::memcpy(j.grid, plan->dims, sizeof(j.grid));
   j.ms = ms;
@@ -2075,13 +2077,8 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
                                       lincomb_chunks((long long)(ks + 1) / 2 * ns)});
     b->n_lincomb += (j.nA > 0) + (j.nB > 0);
   }
-  j.tiles_m = (ms + fmm::BM - 1) / fmm::BM;
   j.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
   j.chunks = batch_chunks(plan->rank, ks);
-  j.units = j.tiles_m * j.tiles_n * j.chunks;
-  j.ticket_off = b->n_tickets;
-  if (j.chunks > 1) b->n_tickets += (size_t)j.tiles_m * j.tiles_n;
-  j.cost = (double)plan->rank / j.chunks * ((ks + fmm::BK - 1) / fmm::BK);
   // direct staging: operands are single unit-coefficient blocks (pre-summed or classical)
   // and every k step stays inside them
   if (!((j.presum || plan->rank == 1) && whole_k_steps(j.grid, j.kk))) b->direct[phase] = false;
@@ -2108,10 +2105,13 @@ void batch_free(fmm_batch* b) {
 // The host side of a batch: jobs per phase in scheduling order, unit ranges, and the sizes
 // of the tickets and workspaces.  Allocates no device memory (the plans' tables are
 // uploaded on first use by device_tables).
-int batch_build(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
+int batch_build(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out,
+                const int* tile_m = nullptr) {
   if (!out || count <= 0 || !m || !n || !k) return FMM_E_INVALID;
-  for (int i = 0; i < count; ++i)
+  for (int i = 0; i < count; ++i) {
     if (m[i] < 0 || n[i] < 0 || k[i] < 0) return FMM_E_INVALID;
+    if (tile_m && tile_m[i] != 0 && tile_m[i] != fmm::BM && tile_m[i] != fmm::BM / 2) return FMM_E_INVALID;
+  }
   int dev = 0;
   int rc = batch_configure(&dev);
   if (rc != FMM_OK) return rc;
@@ -2127,6 +2127,7 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
     const fmm_plan* p = (plans && plans[i]) ? plans[i] : nullptr;
     b->plans.push_back(p);
     const bool live = m[i] > 0 && n[i] > 0 && k[i] > 0;
+    const int bm = (tile_m && tile_m[i] != 0) ? tile_m[i] : fmm::BM;
     auto reserve = [&](int rows, int cols) {
       const size_t off = b->pitch_bytes;
       b->pitch_bytes += (sizeof(double) * (size_t)(rows + 1) * cols + 255) & ~(size_t)255;
@@ -2136,7 +2137,7 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
     b->pitch_b.push_back(live && (k[i] & 1) ? reserve(k[i], n[i]) : SIZE_MAX);
     if (!live) continue;
     if (!p) {
-      batch_add_job(b, 0, i, cls, m[i], n[i], k[i], 0, 0, 0, 0, 0, 0);
+      batch_add_job(b, 0, i, cls, m[i], n[i], k[i], 0, 0, 0, 0, 0, 0, bm);
       continue;
     }
     // same partition and fringe regions as the single-problem path (run_fmm + peel)
@@ -2144,11 +2145,22 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
     const int mr = m[i] % pm, kr = k[i] % pk, nr = n[i] % pn;
     const int md = m[i] - mr, kd = k[i] - kr, nd = n[i] - nr;
     if (md > 0 && nd > 0 && kd > 0)
-      batch_add_job(b, 0, i, p, md / p->dims[0], nd / p->dims[2], kd / p->dims[1], 0, 0, 0, 0, 0, 0);
-    if (kr > 0 && md > 0 && nd > 0) batch_add_job(b, 1, i, cls, md, nd, kr, 0, kd, kd, 0, 0, 0);
-    if (nr > 0) batch_add_job(b, 0, i, cls, m[i], nr, k[i], 0, 0, 0, nd, 0, nd);
-    if (mr > 0 && nd > 0) batch_add_job(b, 0, i, cls, mr, nd, k[i], md, 0, 0, 0, md, 0);
+      batch_add_job(b, 0, i, p, md / p->dims[0], nd / p->dims[2], kd / p->dims[1], 0, 0, 0, 0, 0, 0, bm);
+    if (kr > 0 && md > 0 && nd > 0) batch_add_job(b, 1, i, cls, md, nd, kr, 0, kd, kd, 0, 0, 0, bm);
+    if (nr > 0) batch_add_job(b, 0, i, cls, m[i], nr, k[i], 0, 0, 0, nd, 0, nd, bm);
+    if (mr > 0 && nd > 0) batch_add_job(b, 0, i, cls, mr, nd, k[i], md, 0, 0, 0, md, 0, bm);
   }
+  // Tile heights (64-row tiles only where the whole phase runs the direct variant), then
+  // each job's units and tickets.
+  for (int ph = 0; ph < 2; ++ph)
+    for (auto& j : b->jobs[ph]) {
+      if (!b->direct[ph]) j.bm = fmm::BM;
+      j.tiles_m = (j.ms + j.bm - 1) / j.bm;
+      j.units = j.tiles_m * j.tiles_n * j.chunks;
+      j.ticket_off = b->n_tickets;
+      if (j.chunks > 1) b->n_tickets += (size_t)j.tiles_m * j.tiles_n;
+      j.cost = (double)j.plan->rank / j.chunks * ((j.ks + fmm::BK - 1) / fmm::BK) * j.bm / fmm::BM;
+    }
   // Longest units first: the persistent grid takes units in order, so the short ones
   // fill in at the end.
   for (int ph = 0; ph < 2; ++ph) {
@@ -2177,9 +2189,10 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
   return FMM_OK;
 }
 
-int batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out) {
+int batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k, fmm_batch** out,
+                 const int* tile_m = nullptr) {
   fmm_batch* b = nullptr;
-  int rc = batch_build(count, plans, m, n, k, &b);
+  int rc = batch_build(count, plans, m, n, k, &b, tile_m);
   if (rc != FMM_OK) return rc;
   auto fail = [&](cudaError_t e) {
     batch_free(b);
@@ -2233,6 +2246,7 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
     a.ks = j.ks;
     a.nprod = j.plan->rank;
     a.tiles_m = j.tiles_m;
+    a.bm = j.bm;
     a.tiles_n = j.tiles_n;
     a.chunks = j.chunks;
     a.mode = fmm::MODE_ACCUM_C;
@@ -2427,6 +2441,11 @@ extern "C" {
 int fmm_batch_create(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k,
                      fmm_batch** out) {
   return batch_create(count, plans, m, n, k, out);
+}
+
+int fmm_batch_create_tiled(int count, const fmm_plan* const* plans, const int* m, const int* n, const int* k,
+                           const int* tile_m, fmm_batch** out) {
+  return batch_create(count, plans, m, n, k, out, tile_m);
 }
 
 int fmm_batch_dgemm(fmm_batch* batch, const double* const* A, const long* lda, const double* const* B,

@@ -89,6 +89,9 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_split_gemm_dev.restype = c_int
     lib.fmm_batch_create.argtypes = [c_int, ctypes.POINTER(c_void_p), c_int_p, c_int_p, c_int_p, ctypes.POINTER(c_void_p)]
     lib.fmm_batch_create.restype = c_int
+    lib.fmm_batch_create_tiled.argtypes = [c_int, ctypes.POINTER(c_void_p), c_int_p, c_int_p, c_int_p, c_int_p,
+                                           ctypes.POINTER(c_void_p)]
+    lib.fmm_batch_create_tiled.restype = c_int
     lib.fmm_batch_dgemm.argtypes = [c_void_p, ctypes.POINTER(c_void_p), ctypes.POINTER(c_long), ctypes.POINTER(c_void_p),
                                     ctypes.POINTER(c_long), ctypes.POINTER(c_void_p), ctypes.POINTER(c_long), c_void_p]
     lib.fmm_batch_dgemm.restype = c_int
@@ -276,9 +279,10 @@ class Batch:
     allocates the job tables, tickets and pre-summed operand workspaces once.  `run`
     then takes this call's operands (column-major float64 CUDA tensors) and enqueues
     the launch on the current stream; it can be captured in a CUDA graph (the graph
-    replays with the operand pointers of the captured call)."""
+    replays with the operand pointers of the captured call).  `tiles[i]` is problem i's
+    tile height, 128 (default) or 64 rows (fmm_batch_create_tiled)."""
 
-    def __init__(self, shapes, plans=None):
+    def __init__(self, shapes, plans=None, tiles=None):
         self._lib = load_library()
         shapes = [tuple(int(v) for v in s) for s in shapes]
         if not shapes:
@@ -288,11 +292,18 @@ class Batch:
         if len(plans) != count:
             raise FmmError(-1, "plans and shapes differ in length")
         self.shapes, self.plans = shapes, plans
+        self.tiles = [int(t) for t in tiles] if tiles is not None else None
+        if self.tiles is not None and len(self.tiles) != count:
+            raise FmmError(-1, "tiles and shapes differ in length")
         ci = ctypes.c_int * count
         handles = (ctypes.c_void_p * count)(*[p.handle if p is not None else None for p in plans])
         h = ctypes.c_void_p()
-        _check(self._lib.fmm_batch_create(count, handles, ci(*[s[0] for s in shapes]), ci(*[s[1] for s in shapes]),
-                                          ci(*[s[2] for s in shapes]), ctypes.byref(h)), "fmm_batch_create")
+        dims = (ci(*[s[0] for s in shapes]), ci(*[s[1] for s in shapes]), ci(*[s[2] for s in shapes]))
+        if self.tiles is None:
+            _check(self._lib.fmm_batch_create(count, handles, *dims, ctypes.byref(h)), "fmm_batch_create")
+        else:
+            _check(self._lib.fmm_batch_create_tiled(count, handles, *dims, ci(*self.tiles), ctypes.byref(h)),
+                   "fmm_batch_create_tiled")
         self.handle = h
 
     def units(self, phase: int = 0) -> int:

@@ -224,11 +224,15 @@ class TuneReport:
     choices: List[str]
     model_choices: List[str]
     trials: List[Tuple[str, float]] = field(default_factory=list)  # (description, measured ms)
+    tiles: List[int] = field(default_factory=list)  # tile height per problem (128 or 64 rows)
 
     def counts(self) -> Dict[str, int]:
+        """Problems per (algorithm, tile height), e.g. {"classical/128": 500, "222-1/64": 3}."""
         out: Dict[str, int] = {}
-        for c in self.choices:
-            out[c] = out.get(c, 0) + 1
+        tiles = self.tiles or [TILE] * len(self.choices)
+        for c, t in zip(self.choices, tiles):
+            key = f"{c}/{t}"
+            out[key] = out.get(key, 0) + 1
         return out
 
 
@@ -293,7 +297,33 @@ class BatchTuner:
             if not improved:
                 break
         rep.choices = list(choices)
+        # tile height: 64-row tiles halve a problem's unit length (twice the units); they help
+        # where a problem's units are long and few, so the batch's last units finish late.  The
+        # model ranks problems by unit length over unit count; the measurement decides.
+        rep.tiles = [TILE] * len(shapes)
+        order = sorted(range(len(shapes)), key=lambda i: -self.tile_pressure(choices[i], shapes[i]))
+        for frac in (0.05, 0.25, 1.0):
+            sel = order[:max(1, int(round(frac * len(order))))]
+            trial = list(rep.tiles)
+            for i in sel:
+                trial[i] = TILE // 2
+            t = measure(choices, trial)
+            rep.trials.append((f"64-row tiles for {len(sel)} problems", t))
+            if t < best * 0.995:
+                best, rep.tiles = t, trial
         return rep
+
+    def tile_pressure(self, name: str, shape: Sequence[int]) -> float:
+        """k steps per unit over units: large for problems with long, few units."""
+        m, n, k = shape
+        plan = plan_of(name)
+        if plan is None:
+            ms, ns, ks, R = m, n, k, 1
+        else:
+            p = algebra.partition(m, n, k, plan.dims)
+            ms, ns, ks, R = max(p.ms, 1), max(p.ns, 1), max(p.ks, 1), plan.rank
+        units = _tiles(ms, ns) * R
+        return (ks / KSTEP) / max(units, 1)
 
 
 def random_batch_shapes(count: int = 512, lo: int = 256, hi: int = 4096, seed: int = 0) -> List[Tuple[int, int, int]]:
@@ -304,8 +334,9 @@ def random_batch_shapes(count: int = 512, lo: int = 256, hi: int = 4096, seed: i
 
 
 def batch_timer(runtime, shapes, As, Bs, Cs, reps: int = 3, warmup: int = 1):
-    """measure(choices) for BatchTuner: builds a Batch with the named plans and returns the
-    best of `reps` device-timed runs in milliseconds.  The runs add into Cs."""
+    """measure(choices, tiles=None) for BatchTuner: builds a Batch with the named plans (and
+    per-problem tile heights) and returns the best of `reps` device-timed runs in
+    milliseconds.  The runs add into Cs."""
     import torch
 
     plans: Dict[str, object] = {}
@@ -317,8 +348,8 @@ def batch_timer(runtime, shapes, As, Bs, Cs, reps: int = 3, warmup: int = 1):
             plans[name] = runtime.Plan.from_levels(*candidate_levels(name))
         return plans[name]
 
-    def measure(choices: Sequence[str]) -> float:
-        b = runtime.Batch(shapes, [plan(c) for c in choices])
+    def measure(choices: Sequence[str], tiles: Optional[Sequence[int]] = None) -> float:
+        b = runtime.Batch(shapes, [plan(c) for c in choices], tiles=tiles)
         try:
             for _ in range(warmup):
                 b.run(As, Bs, Cs)

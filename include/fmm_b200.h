@@ -191,6 +191,14 @@ int fmm_split_gemm_dev(const fmm_plan *plan, int m, int n, int k, const float *A
 typedef struct fmm_batch fmm_batch;
 int fmm_batch_create(int count, const fmm_plan *const *plans, const int *m, const int *n, const int *k,
                      fmm_batch **out);
+/* The same with a tile height per problem: tile_m[i] = 128 (the default, also 0) or 64 rows per
+ * work unit (problem i's FMM core and fringe strips).  64-row tiles halve a problem's unit
+ * length and double its unit count (a finer split of the batch's work over the SMs); they run
+ * in phases of the direct variant (pre-summed or classical jobs) and fall back to 128 rows
+ * elsewhere.  Results of a 64-row problem equal a single call's up to rounding (two partial k
+ * sums per tile), not bit for bit. */
+int fmm_batch_create_tiled(int count, const fmm_plan *const *plans, const int *m, const int *n, const int *k,
+                           const int *tile_m, fmm_batch **out);
 int fmm_batch_dgemm(fmm_batch *batch, const double *const *A, const long *lda, const double *const *B,
                     const long *ldb, double *const *C, const long *ldc, void *stream);
 /* A batch formed, run and released in one stream-ordered call, for request loops that

@@ -149,3 +149,35 @@ def test_batch_rejects_mismatched_operands():
     with pytest.raises(rt.FmmError):
         batch.run([A], [A], [A])
     batch.close()
+
+
+def test_batch_with_64_row_tiles_matches_oracle(oracle_lib):
+    """Per-problem tile heights (fmm_batch_create_tiled): 64-row problems split each tile's
+    k steps over the two rows of consumer warps, so they agree with the oracle to rounding."""
+    shapes = [(700, 500, 640), (2048, 2048, 2048), (300, 257, 512), (1030, 1001, 777)]
+    names = [None, "222-1", None, "222-1"]
+    tiles = [64, 64, 128, 64]
+    rngs = [np.random.default_rng(40 + i) for i in range(len(shapes))]
+    host = [(np.asfortranarray(r.uniform(-1, 1, (m, k))), np.asfortranarray(r.uniform(-1, 1, (k, n))),
+             np.asfortranarray(r.uniform(-1, 1, (m, n)))) for r, (m, n, k) in zip(rngs, shapes)]
+    dev = [tuple(rt.colmajor(*x.shape, device=DEV).copy_(torch.from_numpy(x)) for x in h) for h in host]
+    batch = rt.Batch(shapes, [plan_for(nm) for nm in names], tiles=tiles)
+    batch.run([d[0] for d in dev], [d[1] for d in dev], [d[2] for d in dev])
+    torch.cuda.synchronize()
+    batch.close()
+    assert rt.load_library().fmm_device_status(1) == 0
+    for (m, n, k), nm, (A, B, C), d in zip(shapes, names, host, dev):
+        want = C.copy(order="F")
+        if nm is None:
+            oracle_lib.bl_dgemm(A, B, want)
+        else:
+            pl = plan_for(nm).algebra
+            dims, nterms, rows, cols, coefs = rt.plan_tables(pl)
+            oracle_lib.fmm((dims, pl.rank, nterms, rows, cols, coefs), "abc", A, B, want)
+        got = d[2].cpu().numpy()
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-13, (m, n, k, nm)
+
+
+def test_batch_rejects_unknown_tile_height():
+    with pytest.raises(rt.FmmError):
+        rt.Batch([(64, 64, 64)], tiles=[96])

@@ -49,7 +49,7 @@ def test_search_keeps_measured_improvements():
     shapes = [(4096, 4096, 4096)] * 4 + [(300, 300, 300)] * 4
     calls = []
 
-    def measure(choices):  # a machine on which every FMM is slower than classical
+    def measure(choices, tiles=None):  # a machine on which every FMM is slower than classical
         calls.append(list(choices))
         return sum(2.0 if c != "classical" else 1.0 for c in choices)
 
@@ -119,3 +119,26 @@ def test_single_problem_view_adds_waves_and_launches():
     a = tuner.model_time_single(m, "222-1", 16384, 16384, 16384)
     b = tuner.model_time(m, "222-1", 16384, 16384, 16384)
     assert abs(a / b - 1) < 0.05
+
+
+def test_tile_refinement_keeps_64_row_tiles_only_where_measured_faster():
+    """The tuner tries 64-row tiles for the problems with the longest, fewest units first and
+    keeps a tile choice only when the measured batch gets faster."""
+    shapes = [(256, 256, 4096)] * 2 + [(2048, 2048, 512)] * 38
+    tn = tuner.BatchTuner()
+    pressure = [tn.tile_pressure("classical", s) for s in shapes]
+    assert min(pressure[:2]) > max(pressure[2:])  # deep, narrow problems rank first
+
+    def measure(choices, tiles=None):  # 64-row tiles help the two deep problems only
+        t = 100.0
+        for i, tl in enumerate(tiles or [128] * len(choices)):
+            if tl == 64:
+                t += -3.0 if i < 2 else 1.0
+        return t
+
+    rep = tn.tune(shapes, measure)
+    assert rep.tiles[:2] == [64, 64] and set(rep.tiles[2:]) == {128}
+    assert rep.counts()["classical/64"] == 2
+
+    rep2 = tn.tune(shapes, lambda c, tiles=None: 100.0 + sum(1.0 for x in (tiles or []) if x == 64))
+    assert set(rep2.tiles) == {128}
