@@ -678,6 +678,8 @@ int launch_gemm(int kind, const fmm::Prod* prods, const fmm::Term* terms, const 
 
 const int kUnitGrid[3] = {1, 1, 1};
 
+int call_ksplit(const fmm_plan* plan, int ms, int ns, int ks, bool presum, int kk, int nsm);  // below
+
 int sm_count_current() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
@@ -693,8 +695,7 @@ int plain_gemm(int m, int n, int k, const double* A, long long lda, const double
   int dev = 0;
   rc = configure_kernel(&dev);
   if (rc != FMM_OK) return rc;
-  const long long tiles = (long long)((m + fmm::BM - 1) / fmm::BM) * ((n + fmm::BN - 1) / fmm::BN);
-  const int S = choose_ksplit(tiles, k, sm_count[dev]);
+  const int S = call_ksplit(classical_plan(), m, n, k, false, k, sm_count[dev]);
   if (S > 1) {
     const fmm::Prod* vp = nullptr;
     const fmm::Term* vt = nullptr;
@@ -778,12 +779,14 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
   ca.nterms = plan->n_cterms;
   ca.grid_m = plan->dims[0];
   ca.grid_n = plan->dims[2];
-  const size_t smem = fmm::combine_smem_bytes(ca.grid_m * ca.grid_n, ca.nterms, ca.nprod);
-  const long long blocks = ((long long)ms * ns + fmm::COMBINE_THREADS - 1) / fmm::COMBINE_THREADS;
-  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 8));
+  // many C blocks: smaller CTAs, so that more of them (and more loads in flight) fit per SM
+  const int threads = ca.grid_m * ca.grid_n > 16 ? fmm::COMBINE_THREADS / 2 : fmm::COMBINE_THREADS;
+  const size_t smem = fmm::combine_smem_bytes(ca.grid_m * ca.grid_n, ca.nterms, ca.nprod, threads);
+  const long long blocks = ((long long)ms * ns + threads - 1) / threads;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 16));
   {
     ProfScope pf(K_COMBINE, st);
-    fmm::fmm_combine_kernel<<<grid, fmm::COMBINE_THREADS, smem, st>>>(ca);
+    fmm::fmm_combine_kernel<<<grid, threads, smem, st>>>(ca);
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cuda_status(cudaGetLastError());
@@ -935,6 +938,19 @@ size_t presum_bytes(const fmm_plan* plan, int ms, int ns, int ks) {
          16;
 }
 
+// The k split a single call gives products of ms x ks x ns: the pre-summed direct launch
+// (unless the call stores its products or runs them in workspace groups) and the classical
+// plan split as choose_ksplit decides; other forms keep S = 1.  Batches apply the same split
+// per job.
+int call_ksplit(const fmm_plan* plan, int ms, int ns, int ks, bool presum, int kk, int nsm) {
+  const long long tiles = (long long)((ms + fmm::BM - 1) / fmm::BM) * ((ns + fmm::BN - 1) / fmm::BN);
+  if (plan->rank == 1) return choose_ksplit(tiles, ks, nsm);
+  if (!presum) return 1;
+  if (combine_fits(plan) && prefer_stored_products(plan, ms, ns, ks)) return 1;
+  if ((long long)presum_bytes(plan, ms, ns, ks) > g_ws_limit.load()) return 1;
+  return choose_ksplit(tiles * plan->rank, kk, nsm);
+}
+
 // Pre-summed products in groups, when one call's whole operand workspace would exceed the
 // workspace limit: the R products run as groups of G consecutive products, each group's
 // operand sums (one slot per product, k extent padded to whole k steps) formed into one of
@@ -1065,8 +1081,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         t_last_ws = (long long)presum_bytes(plan, ms, ns, ks);
         PresumPlan pp;
         rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
-        const long long units = (long long)((ms + fmm::BM - 1) / fmm::BM) * ((ns + fmm::BN - 1) / fmm::BN) * R;
-        const int S = choose_ksplit(units, pp.kk, sm_count_current());
+        const int S = call_ksplit(plan, ms, ns, ks, true, pp.kk, sm_count_current());
         const fmm::Prod* vp = pp.prods;
         const fmm::Term* vt = pp.terms;
         if (rc == FMM_OK && S > 1) rc = ksplit_tables(plan, pp.kk != ks ? BASE_ALL : BASE_PS, S, &vp, &vt);
@@ -1980,6 +1995,9 @@ struct fmm_batch {
     long long ldT;
     int chunks, tiles_m, tiles_n, units;
     int bm;                        // tile height: fmm::BM, or BM / 2 (direct phases only)
+    int S;                         // k split of the job's products (the one a single call chooses)
+    const fmm::Prod* vprods;       // its k-split tables when S > 1
+    const fmm::Term* vterms;
     size_t ticket_off;             // int offset into the ticket array
     double cost;                   // estimated k steps per unit (scheduling order)
   };
@@ -2078,7 +2096,10 @@ void batch_add_job(fmm_batch* b, int phase, int prob, const fmm_plan* plan, int 
     b->n_lincomb += (j.nA > 0) + (j.nB > 0);
   }
   j.tiles_n = (ns + fmm::BN - 1) / fmm::BN;
-  j.chunks = batch_chunks(plan->rank, ks);
+  // the k split a single call gives these products, so a batch computes each problem with the
+  // same arithmetic as a call of its own
+  j.S = call_ksplit(plan, ms, ns, ks, j.presum, j.kk, sm_count[b->dev]);
+  j.chunks = batch_chunks(plan->rank * j.S, j.kk / j.S);
   // direct staging: operands are single unit-coefficient blocks (pre-summed or classical)
   // and every k step stays inside them
   if (!((j.presum || plan->rank == 1) && whole_k_steps(j.grid, j.kk))) b->direct[phase] = false;
@@ -2159,7 +2180,7 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
       j.units = j.tiles_m * j.tiles_n * j.chunks;
       j.ticket_off = b->n_tickets;
       if (j.chunks > 1) b->n_tickets += (size_t)j.tiles_m * j.tiles_n;
-      j.cost = (double)j.plan->rank / j.chunks * ((j.ks + fmm::BK - 1) / fmm::BK) * j.bm / fmm::BM;
+      j.cost = (double)j.plan->rank / j.chunks * ((j.kk + fmm::BK - 1) / fmm::BK) * j.bm / fmm::BM;
     }
   // Longest units first: the persistent grid takes units in order, so the short ones
   // fill in at the end.
@@ -2179,6 +2200,9 @@ int batch_build(int count, const fmm_plan* const* plans, const int* m, const int
     for (auto& j : b->jobs[ph]) {
       DevTables* d = nullptr;
       rc = device_tables(j.plan, &d);
+      if (rc == FMM_OK && j.S > 1)
+        rc = ksplit_tables(j.plan, j.plan->rank == 1 ? BASE_ORIG : (j.kk != j.ks ? BASE_ALL : BASE_PS), j.S,
+                           &j.vprods, &j.vterms);
       if (rc != FMM_OK) {
         batch_free(b);
         return rc;
@@ -2308,6 +2332,12 @@ bool batch_fill(fmm_batch* b, int ph, const double* const* A, const long* lda, c
            make_tensor_map(&a.tmBw2, a.Bw, j.kk, (long long)j.nB * j.ns, j.ldT, fmm::TB_K, fmm::BN);
     else
       a.tmBw = a.tmB, a.tmBw2 = a.tmB2;
+    if (j.S > 1) {  // the k-split tables (part depth kk / S); the tensor maps keep the full depth
+      a.ks /= j.S;
+      a.nprod *= j.S;
+      a.prods = j.vprods;
+      a.terms = j.vterms;
+    }
     tma = tma && ok;
     b->h_jobs[ph][q] = a;
   }

@@ -293,10 +293,11 @@ __device__ __forceinline__ int prod_T(const Prod& p) { return p.na > p.nb ? p.na
 
 // Work unit u -> (tile position, product range).  Chunk-major order: the units of one tile
 // are a whole tile grid apart, so a later chunk is claimed well after the earlier one.
-// rows: the tile's rows inside the block (at most the tile height).  half: the tile has at
-// most BM / 2 rows (a job of half-height tiles, or the last tile row of a block whose height
-// leaves <= 64 rows there); the direct variant then stages a BM / 2-row box of A and lets
-// both rows of consumer warps cover those rows, taking alternate k steps.
+// unit_rows: the tile's rows inside the block (at most the tile height).  unit_half: the tile
+// has at most BM / 2 rows (a job of half-height tiles, or the last tile row of a block whose
+// height leaves <= 64 rows there); the direct variant then stages a BM / 2-row box of A and
+// lets both rows of consumer warps cover those rows, each taking half of the column fragments
+// (every element still gets a full tile's DMMAs in the same order).
 struct Unit {
   int m0, n0, tile, r0, r1;
 };
@@ -926,9 +927,10 @@ __device__ __forceinline__ void frag_counts(int vr, int vc, int wm, int wn, int&
 // the whole 64 x 32 warp tile; fewer for the warps of an edge tile, whose other
 // fragments stay as they were and are never written out).  Compile-time counts keep each
 // form straight-line code: shared-memory loads and DMMAs with no predicates.
+// jb: first column fragment (the half-height form gives each row of warps two of the four).
 template <int IM, int JN, int LDA = LDA_S>
 __device__ __forceinline__ void mma_stage_t(const double* opA, const double* opB, double (&acc)[4][4][4], int wm,
-                                            int wn, int g, int t4) {
+                                            int wn, int g, int t4, int jb = 0) {
 #pragma unroll
   for (int kq = 0; kq < BK / 4; ++kq) {
     double af[4][2], bf[4];
@@ -939,7 +941,7 @@ __device__ __forceinline__ void mma_stage_t(const double* opA, const double* opB
       af[i][1] = opA[(kq * 4 + t4) * LDA + row + 8];
     }
 #pragma unroll
-    for (int j = 0; j < JN; ++j) bf[j] = opB[(frag_col(wn, j) + g) * LDB_S + kq * 4 + t4];
+    for (int j = 0; j < JN; ++j) bf[j] = opB[(frag_col(wn, jb + j) + g) * LDB_S + kq * 4 + t4];
 #pragma unroll
     for (int i = 0; i < IM; ++i)
 #pragma unroll
@@ -1266,15 +1268,15 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
 #pragma unroll
           for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
       if (half) {
-        // both rows of warps on the tile's BM / 2 rows, warp row wm taking the k steps s with
-        // s % 2 == wm; every warp still waits for each stage before releasing it, so no
-        // release can land in the stage's previous phase
+        // both rows of warps on the tile's BM / 2 rows, warp row wm taking the column
+        // fragments 2 wm, 2 wm + 1 of its warp column: each element gets the DMMAs of a full
+        // tile in the same order (results equal a full tile's bit for bit), in half the time
 #pragma unroll 1
         for (int s = 0; s < nks; ++s, ++kc) {
           const int stage = (int)(kc % NSTAGE_D);
           const double* opA = stages + (size_t)stage * STAGE_SZ;
           mbar_wait(full0 + 8 * stage, (unsigned)((kc / NSTAGE_D) & 1), src.status());
-          if ((s & 1) == wm) mma_stage_t<4, 4, BM / 2>(opA, opA + OPA_SZ, acc, 0, wn, g, t4);
+          mma_stage_t<4, 2, BM / 2>(opA, opA + OPA_SZ, acc, 0, wn, g, t4, 2 * wm);
           __threadfence_block();
           __syncwarp();
           if (lane == 0) mbar_arrive(empty0 + 8 * stage);
@@ -1296,30 +1298,16 @@ __device__ __forceinline__ void direct_consumer(const Src& src, const double* st
       }
       // hand the product tile to the epilogue warps once they are done with the previous one
       mbar_wait(mempty, (unsigned)((q & 1) ^ 1), src.status());
-      if (half) {  // rows 0..63: warp row 0's sums, then warp row 1's added
-        if (wm == 0) {
+      if (half) {  // rows 0..63, this warp's two column fragments
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < 2; ++j)
 #pragma unroll
-              for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < 2; ++h)
 #pragma unroll
-                for (int e = 0; e < 2; ++e)
-                  Ms[(frag_col(wn, j) + t4 * 2 + e) * MS_LD + i * 16 + g + 8 * h] = acc[i][j][2 * h + e];
-        }
-        named_bar_sync(3, NCONS);
-        if (wm == 1) {
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-              for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int e = 0; e < 2; ++e)
-                  Ms[(frag_col(wn, j) + t4 * 2 + e) * MS_LD + i * 16 + g + 8 * h] += acc[i][j][2 * h + e];
-        }
+              for (int e = 0; e < 2; ++e)
+                Ms[(frag_col(wn, 2 * wm + j) + t4 * 2 + e) * MS_LD + i * 16 + g + 8 * h] = acc[i][j][2 * h + e];
       } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -1619,20 +1607,22 @@ struct CombineArgs {
   int grid_m, grid_n;  // C block grid
 };
 
-constexpr int COMBINE_THREADS = 256;
+constexpr int COMBINE_THREADS = 256;  // threads per CTA (128 when the plan has more than 16 C blocks)
 constexpr int COMBINE_MAX_BLOCKS = 64;
 constexpr int COMBINE_MAX_TERMS = 4096;
 constexpr int COMBINE_BATCH = 8;
+constexpr int COMBINE_TERMS = 4;  // C terms of one product updated together (their blocks differ)
 
-__host__ __device__ constexpr size_t combine_smem_bytes(int nblk, int nterms, int nprod) {
-  return sizeof(double) * (size_t)nblk * COMBINE_THREADS + (sizeof(double) + sizeof(int)) * (size_t)nterms +
+__host__ __device__ constexpr size_t combine_smem_bytes(int nblk, int nterms, int nprod, int threads = COMBINE_THREADS) {
+  return sizeof(double) * (size_t)nblk * threads + (sizeof(double) + sizeof(int)) * (size_t)nterms +
          sizeof(int) * (size_t)(nprod + 1);
 }
 
 __global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const CombineArgs a) {
   extern __shared__ __align__(16) double cacc[];
+  const int nt = blockDim.x;
   const int nblk = a.grid_m * a.grid_n;
-  double* tcoef = cacc + (size_t)nblk * COMBINE_THREADS;
+  double* tcoef = cacc + (size_t)nblk * nt;
   int* tblk = reinterpret_cast<int*>(tcoef + a.nterms);
   int* tfirst = tblk + a.nterms;  // compact C-term ranges per product, nprod + 1 entries
   if (threadIdx.x == 0) {
@@ -1644,7 +1634,7 @@ __global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const Comb
     tfirst[a.nprod] = acc;
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < a.nprod; r += blockDim.x) {
+  for (int r = threadIdx.x; r < a.nprod; r += nt) {
     const Prod p = a.prods[r];
     for (int c = 0; c < p.nc; ++c) {
       const Term t = a.terms[p.c0 + c];
@@ -1655,7 +1645,7 @@ __global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const Comb
   __syncthreads();
   const int tid = threadIdx.x;
   const long long total = (long long)a.ms * a.ns;
-  for (long long e0 = (long long)blockIdx.x * COMBINE_THREADS; e0 < total; e0 += (long long)gridDim.x * COMBINE_THREADS) {
+  for (long long e0 = (long long)blockIdx.x * nt; e0 < total; e0 += (long long)gridDim.x * nt) {
     const long long e = e0 + tid;
     if (e >= total) continue;
     const int i = (int)(e % a.ms);
@@ -1672,7 +1662,7 @@ __global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const Comb
       }
 #pragma unroll
       for (int q = 0; q < COMBINE_BATCH; ++q)
-        if (b0 + q < nblk) cacc[(size_t)(b0 + q) * COMBINE_THREADS + tid] = v[q];
+        if (b0 + q < nblk) cacc[(size_t)(b0 + q) * nt + tid] = v[q];
     }
     for (int r0 = 0; r0 < a.nprod; r0 += COMBINE_BATCH) {
       double m[COMBINE_BATCH];
@@ -1683,15 +1673,27 @@ __global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const Comb
       for (int q = 0; q < COMBINE_BATCH; ++q) {
         const int r = r0 + q;
         if (r >= a.nprod) break;
-        for (int c = tfirst[r]; c < tfirst[r + 1]; ++c) {
-          double* x = cacc + (size_t)tblk[c] * COMBINE_THREADS + tid;
-          *x = fma(tcoef[c], m[q], *x);
+        // a product's C terms name distinct blocks: their values are read together, then
+        // updated and written back, instead of one dependent read-update-write per term
+        for (int c = tfirst[r]; c < tfirst[r + 1]; c += COMBINE_TERMS) {
+          double x[COMBINE_TERMS], w[COMBINE_TERMS];
+          double* px[COMBINE_TERMS];
+#pragma unroll
+          for (int t = 0; t < COMBINE_TERMS; ++t) {
+            const bool ok = c + t < tfirst[r + 1];
+            px[t] = cacc + (size_t)(ok ? tblk[c + t] : 0) * nt + tid;
+            w[t] = ok ? tcoef[c + t] : 0.0;
+            x[t] = ok ? *px[t] : 0.0;
+          }
+#pragma unroll
+          for (int t = 0; t < COMBINE_TERMS; ++t)
+            if (c + t < tfirst[r + 1]) *px[t] = fma(w[t], m[q], x[t]);
         }
       }
     }
     for (int b = 0; b < nblk; ++b) {
       const int br = b / a.grid_n, bc = b % a.grid_n;
-      a.C[(long long)br * a.ms + i + ((long long)bc * a.ns + j) * a.ldc] = cacc[(size_t)b * COMBINE_THREADS + tid];
+      a.C[(long long)br * a.ms + i + ((long long)bc * a.ns + j) * a.ldc] = cacc[(size_t)b * nt + tid];
     }
   }
 }

@@ -152,8 +152,9 @@ def test_batch_rejects_mismatched_operands():
 
 
 def test_batch_with_64_row_tiles_matches_oracle(oracle_lib):
-    """Per-problem tile heights (fmm_batch_create_tiled): 64-row problems split each tile's
-    k steps over the two rows of consumer warps, so they agree with the oracle to rounding."""
+    """Per-problem tile heights (fmm_batch_create_tiled): a 64-row tile gives each row of
+    consumer warps half of its columns, every element getting a full tile's DMMAs in order, so
+    the results match the oracle and equal single calls bit for bit."""
     shapes = [(700, 500, 640), (2048, 2048, 2048), (300, 257, 512), (1030, 1001, 777)]
     names = [None, "222-1", None, "222-1"]
     tiles = [64, 64, 128, 64]
@@ -166,7 +167,10 @@ def test_batch_with_64_row_tiles_matches_oracle(oracle_lib):
     torch.cuda.synchronize()
     batch.close()
     assert rt.load_library().fmm_device_status(1) == 0
-    for (m, n, k), nm, (A, B, C), d in zip(shapes, names, host, dev):
+    singles = one_by_one(shapes, names, [d[0] for d in dev], [d[1] for d in dev],
+                         [rt.colmajor(*h[2].shape, device=DEV).copy_(torch.from_numpy(h[2])) for h in host])
+    for (m, n, k), nm, (A, B, C), d, w in zip(shapes, names, host, dev, singles):
+        assert torch.equal(d[2], w), (m, n, k, nm)
         want = C.copy(order="F")
         if nm is None:
             oracle_lib.bl_dgemm(A, B, want)

@@ -339,7 +339,7 @@ def test_gpu_ksplit_matches_oracle(oracle_lib, algo, shape):
 
 
 # The last tile row of a block with at most 64 rows runs as a half-height unit in the direct
-# variant (a 64-row A box; both rows of consumer warps on those rows, alternate k steps):
+# variant (a 64-row A box; both rows of consumer warps on those rows, half of the columns each):
 # plain 1050 x 700 x 512 (26-row edge), plain 64 x 300 x 256 (one 64-row tile row), 222-1 at
 # 2100 x 1800 x 1200 (pre-summed, ms = 1048: 24-row edge), 222-1 x 333-1 at 3312 x 2000 x 960
 # (pre-summed, ms = 552: 40-row edge, as at 16384^3).
