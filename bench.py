@@ -402,7 +402,8 @@ def serving_2000(rt, torch, dev, window=1.0, rank=0, world=1):
     out = rep.summary()
     out["arrivals"] = "Poisson 2000 req/s, seed 0" + (f", share of rank {rank}/{world}" if world > 1 else "")
     out["budget_gb"] = 160
-    out["policy"] = "FIFO admission by HBM budget, bounded queue 4096; FP64 requests batched per launch"
+    out["policy"] = ("admission in arrival order by HBM budget, backfill past a waiting request for up to 50 ms, "
+                     "bounded queue 4096; FP64 requests batched per launch")
     del ex
     torch.cuda.empty_cache()
     return out

@@ -10,6 +10,9 @@ of such calls:
   * admission  - a request is admitted when its device bytes (operands plus workspace)
                  fit in the HBM budget beside everything admitted and not yet finished;
                  until then it waits in a bounded queue (arrivals beyond it are rejected).
+                 Requests behind one that does not fit yet may be admitted past it
+                 (backfill) while it has waited less than `head_wait` seconds; after that
+                 admission stops until it fits, so a large request cannot starve.
                  Admission brings its operands into device memory, where they stay until
                  it finishes.
   * batching   - every admitted FP64 request not yet dispatched joins the next FP64 batch:
@@ -178,7 +181,8 @@ class Server:
 
     def __init__(self, executor, budget_bytes: float = 160e9, max_queue: int = 4096, max_batch: int = 512,
                  inflight: int = 2, clock: Callable[[], float] = time.perf_counter,
-                 sleep: Callable[[float], None] = time.sleep):
+                 sleep: Callable[[float], None] = time.sleep, backfill: bool = True, head_wait: float = 0.05,
+                 scan: int = 64):
         self.ex = executor
         self.budget = budget_bytes
         self.max_queue = max_queue
@@ -186,10 +190,13 @@ class Server:
         self.inflight = inflight
         self.clock = clock
         self.sleep = sleep
+        self.backfill = backfill    # admit past a head request that does not fit yet
+        self.head_wait = head_wait  # ... only while it has waited less than this (seconds)
+        self.scan = scan            # queue entries looked at per admission pass
 
     def run(self, requests: Sequence[Request], window: float, drain: bool = True) -> Report:
         reqs = sorted(requests, key=lambda r: r.arrival)
-        queue: deque = deque()
+        queue: List[Request] = []
         ready: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
         running: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
         in_use = peak = 0
@@ -209,14 +216,22 @@ class Server:
                     else:
                         queue.append(reqs[nxt])
                     nxt += 1
-                # admission in arrival order while memory allows
-                while queue and in_use + queue[0].nbytes <= self.budget:
-                    r = queue.popleft()
-                    self.ex.admit(r)
-                    r.admitted = self.clock() - t0
-                    in_use += r.nbytes
-                    peak = max(peak, in_use)
-                    ready[r.kind].append(r)
+                # admission in arrival order while memory allows; past a request that does not
+                # fit yet (backfill) only while that request has waited less than head_wait
+                i = 0
+                while i < len(queue) and i < self.scan:
+                    r = queue[i]
+                    if in_use + r.nbytes <= self.budget:
+                        del queue[i]
+                        self.ex.admit(r)
+                        r.admitted = self.clock() - t0
+                        in_use += r.nbytes
+                        peak = max(peak, in_use)
+                        ready[r.kind].append(r)
+                        continue
+                    if not self.backfill or now - queue[0].arrival > self.head_wait:
+                        break
+                    i += 1
             # dispatch: all ready FP64 requests form one batch; split requests one by one
             for kind in (FP64, SPLIT):
                 while ready[kind] and len(running[kind]) < self.inflight:

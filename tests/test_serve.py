@@ -120,3 +120,41 @@ def test_sharding_is_deterministic_and_balanced():
     model = tuner.B200Model()
     work = [sum(serve.model_cost(model, r) for r in s) for s in a]
     assert max(work) / min(work) < 1.3
+
+
+def _req(rid, kind, shape, alg, t, nbytes):
+    return serve.Request(rid, kind, shape, alg, t, nbytes=int(nbytes))
+
+
+def test_backfill_admits_past_a_request_that_does_not_fit_yet():
+    """A large request that must wait for memory does not hold back the small ones behind it
+    (they are admitted past it), and with head_wait it is admitted once memory frees."""
+    big = [_req(0, serve.FP64, (4096, 4096, 4096), "classical", 0.0, 8e9),
+           _req(1, serve.SPLIT, (8192, 8192, 8192), "222-2", 1e-4, 5e9)]
+    small = [_req(2 + i, serve.FP64, (256, 256, 256), "classical", 2e-4 + 1e-5 * i, 1e7) for i in range(20)]
+    reqs = big + small
+
+    def fresh():
+        return [serve.Request(r.rid, r.kind, r.shape, r.algorithm, r.arrival, nbytes=r.nbytes) for r in reqs]
+
+    rep_fifo, ex_fifo = run(fresh(), 0.5, budget_bytes=10e9, backfill=False)
+    rep_bf, ex_bf = run(fresh(), 0.5, budget_bytes=10e9, backfill=True, head_wait=1.0)
+    # FIFO: every small request is admitted after the split request (which waits for the
+    # first one's memory); with backfill they are admitted before it
+    assert ex_fifo.admitted.index(1) < min(ex_fifo.admitted.index(2 + i) for i in range(20))
+    assert ex_bf.admitted.index(1) > max(ex_bf.admitted.index(2 + i) for i in range(20))
+    assert rep_bf.completed == rep_fifo.completed == len(reqs)
+    small_lat = lambda rep: np.median([r for r in rep.latencies])  # noqa: E731
+    assert small_lat(rep_bf) < small_lat(rep_fifo)
+
+
+def test_backfill_stops_when_the_waiting_request_has_waited_long_enough():
+    """A steady stream of small requests that keeps the budget busy cannot starve a large one:
+    past head_wait nothing is admitted past it, so it gets the memory as launches finish."""
+    first = _req(0, serve.FP64, (4096, 4096, 4096), "classical", 0.0, 6e9)
+    big = _req(1, serve.SPLIT, (8192, 8192, 8192), "222-2", 1e-4, 6e9)
+    small = [_req(2 + i, serve.FP64, (1024, 1024, 1024), "classical", 2e-4 + 2e-4 * i, 2e9) for i in range(400)]
+    rep, ex = run([first, big] + small, 0.2, budget_bytes=10e9, backfill=True, head_wait=0.005)
+    assert 1 in ex.admitted
+    pos = ex.admitted.index(1)
+    assert pos < len(ex.admitted) - 1  # admitted while small requests were still arriving
