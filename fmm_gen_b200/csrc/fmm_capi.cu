@@ -38,7 +38,7 @@ thread_local int t_last_error = FMM_OK;
 int g_ticket_fill = 0;
 // Cap on the pre-summed operand workspace of one call (fmm_set_workspace_limit), and the
 // workspace bytes the last call on this thread used.
-constexpr long long kDefaultWorkspaceLimit = 4LL << 30;
+constexpr long long kDefaultWorkspaceLimit = 8LL << 30;
 std::atomic<long long> g_ws_limit{kDefaultWorkspaceLimit};
 thread_local long long t_last_ws = 0;
 
@@ -1062,6 +1062,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         FMM_CUDA_TRY(cudaMallocAsync((void**)&mws, sizeof(double) * (size_t)mstride * R, st));
         double* M = reinterpret_cast<double*>(mws);
         PresumPlan pp;
+        t_last_ws = (long long)presum_bytes(plan, ms, ns, ks);
         rc = presum_prepare(plan, *d, A, lda, B, ldb, ms, ns, ks, st, &pp);
         if (rc == FMM_OK)
           rc = launch_gemm(K_GEMM_FMM, pp.prods, pp.terms, plan->dims, R, fmm::MODE_STORE_M, A, lda, B, ldb, pp.ps,

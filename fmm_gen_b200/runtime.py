@@ -397,7 +397,7 @@ def bl_dgemm_host(A: np.ndarray, B: np.ndarray, C: np.ndarray) -> None:
 
 
 def set_workspace_limit(nbytes: int) -> int:
-    """Cap one call's pre-summed operand workspace (bytes <= 0: the default, 4 GiB); returns
+    """Cap one call's pre-summed operand workspace (bytes <= 0: the default, 8 GiB); returns
     the previous cap.  Calls that would need more run their products in groups."""
     return int(load_library().fmm_set_workspace_limit(int(nbytes)))
 

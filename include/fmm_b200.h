@@ -110,14 +110,15 @@ int fmm_device_status(int clear);
 /* Workspace of the pre-summed operands (the ABC pack type's large products) -- the
  * reference's counterpart is its packing pool (common/dgemm/bl_dgemm_util.c:375-394),
  * sized by the first call and never bounded.  One call's workspace is capped at `bytes`
- * (default 4 GiB; bytes <= 0 restores it): a call whose sums would need more runs its
+ * (default 8 GiB; bytes <= 0 restores it): a call whose sums would need more runs its
  * products in groups over two halves of a capped workspace, the next group's sums formed
  * while the current group runs; results are unchanged.  The groups' workspace is
  * 2 G (ms + ns) kk 8 bytes for groups of G >= 1 products (kk: the k extent per product
  * rounded up to 8), so a cap below two products' sums is exceeded by that much.  Returns
  * the previous cap.
  * fmm_last_workspace_bytes: pre-summed workspace bytes of the calling thread's last
- * fmm_dgemm_dev / host call (0 when it used none). */
+ * fmm_dgemm_dev / host call (0 when it used none).  The stored products of a call whose C
+ * traffic the library routes through one combine pass (8 R ms ns bytes) are not capped. */
 long long fmm_set_workspace_limit(long long bytes);
 long long fmm_last_workspace_bytes(void);
 

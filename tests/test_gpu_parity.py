@@ -375,7 +375,7 @@ def test_gpu_half_height_edge_tiles(oracle_lib, algo, shape):
 @pytest.mark.parametrize("algs,levels,shape,limit", [
     (["222"], [1], (2048, 2048, 1024), 16 << 20),         # one product per group (2 x 8 MB)
     (["222"], [1], (2048, 2048, 1024), 32 << 20),         # groups of 2 (last group smaller)
-    (["222", "333"], [1, 1], (2000, 2000, 1000), 40 << 20),  # k per product 166: padded slots
+    (["222", "333"], [1, 1], (2400, 2400, 1000), 40 << 20),  # k per product 166: padded slots
 ])
 def test_gpu_presum_groups_match_oracle(oracle_lib, algs, levels, shape, limit):
     m, n, k = shape
