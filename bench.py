@@ -39,11 +39,12 @@ SHAPES = [(16384, 16384, 16384), (14400, 14400, 480), (4000, 16000, 2000)]
 WORKLOAD = "222-1x333-1 abc FP64 C+=A*B over 16384^3, 14400x14400x480, 4000x16000x2000"
 METRIC = "effective TFLOPS (2mnk/t), 222-1x333-1 abc FP64"
 UNIT = "TFLOP/s"
-# DRAM traffic of the FMM products launches per executed core flop, from a one-pass ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum) of one timed step of this workload:
-# 226.9 GB over 6.88e12 executed flops (16384^3: 153.9 GB, 14400x14400x480: 55.7 GB,
-# 4000x16000x2000: 17.3 GB), summarised in profiles/.
-TRAFFIC_BYTES_PER_FLOP = 226.9e9 / 6.88e12
+# DRAM traffic of the FMM products kernel per executed core flop, from a one-pass ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the products launch of a smaller case of
+# the same algorithm, 222-1 x 333-1 at 6144^3: 11.62 GB over 3.46e11 executed flops (its
+# algorithmic bytes: 11.4 GB).  roofline.traffic scales it to the average products launch.
+TRAFFIC_BYTES_PER_FLOP = 11.62e9 / 3.46e11
+TRAFFIC_SOURCE = "scaled by executed flops from one capture of the 222-1x333-1 6144^3 products launch"
 
 
 def effective_flops(shapes):
@@ -642,6 +643,7 @@ def main():
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
                          "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU in this run (FP64 tensor)",
                          "traffic": (TRAFFIC_BYTES_PER_FLOP * per_launch_flops) if TRAFFIC_BYTES_PER_FLOP else None,
+                         "traffic_source": TRAFFIC_SOURCE,
                          "launches": core_launches, "avg_launch_ms": core_ms / max(core_launches, 1),
                          "executed_flops_per_launch": per_launch_flops},
             "kernel_ms": kt.ms, "kernel_launches": kt.count,
