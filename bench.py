@@ -33,6 +33,10 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# torch's tensors and the library's workspaces from one stream-ordered pool (the device's
+# default pool, which the library keeps mapped): the serving measurement fills 160 GB of a
+# 180 GB device, and two separate pools would each hold freed memory the other then lacks.
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "backend:cudaMallocAsync")
 
 ALGS, LEVELS, PACK = ["222", "333"], [1, 1], "abc"
 SHAPES = [(16384, 16384, 16384), (14400, 14400, 480), (4000, 16000, 2000)]

@@ -11,7 +11,7 @@
 //      hi*hi + hi*mid + mid*hi + mid*mid + hi*lo + lo*hi (the dropped ones are ~2^-24
 //      relative), tcgen05.mma kind::f16 into FP32 accumulators in tensor memory: hi*hi
 //      into one, the five smaller products into another, so that the accumulators' own
-//      rounding never drops the small terms against the large ones.  Every 128-deep k
+//      rounding never drops the small terms against the large ones.  Every 256-deep k
 //      chunk is drained with tcgen05.ld (the two accumulators added once in FP32) and
 //      added into FP64 registers, so FP32 rounding only acts within a chunk.  With several
 //      products the epilogue stores M_r (FP64) to a workspace and fmm_combine_kernel adds
@@ -59,7 +59,7 @@ constexpr int NBARS = 2 * NSTG + 2 * NACC + 1;
 constexpr size_t SMEM_BYTES =
     (size_t)NSTG * STAGE_BYTES + 1024 /*alignment slack*/ + 8 * NBARS + 16 /*tensor-memory address*/ + fmm::RING_BYTES;
 constexpr int GROUP_M = 8;
-constexpr int DRAIN_STAGES = 2;                          // stages (of BK) accumulated in FP32 before each FP64 drain
+constexpr int DRAIN_STAGES = 4;                          // stages (of BK) accumulated in FP32 before each FP64 drain
 constexpr int C_PREFETCH_CHUNKS = 4;                     // C tiles go to L2 this many drains before a unit ends
 constexpr int C_BATCH = 16;                              // C elements in flight per thread in the epilogue
 constexpr int LAUNCH_REGS = 65536 / NTHREADS / 8 * 8;    // 168 with one CTA per SM

@@ -163,7 +163,7 @@ int fmm_dgemm_dev_noalloc(const fmm_plan *plan, int m, int n, int k, const doubl
  * enqueued on `stream`.  Same partition, product order and fringe peeling as
  * fmm_dgemm_dev (plan == NULL: classical).  Each product's operand sums are formed in
  * FP64 and split into three bf16 planes; the product is six bf16 plane products
- * accumulated in FP32 over 128-deep k chunks and in FP64 across chunks; W[l,r] * M_r is
+ * accumulated in FP32 over 256-deep k chunks and in FP64 across chunks; W[l,r] * M_r is
  * added to C in FP64.  Relative Frobenius error against the FP64 product of the same
  * FP32 inputs: about 1e-7 (classical) and a few 1e-7 for two Strassen levels.
  * Workspace from the stream-ordered allocator: 6 R (ms + ns) kpad bytes of bf16 planes
