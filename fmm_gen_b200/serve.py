@@ -157,6 +157,7 @@ class Report:
     peak_bytes: int = 0
     run_s: float = 0.0            # the loop's duration (window plus the drain of admitted work)
     stream_busy_s: Dict[str, float] = field(default_factory=dict)  # per stream: device time of its launches
+    host_s: Dict[str, float] = field(default_factory=dict)  # host time in admission, launches, completions
 
     def percentile(self, q: float) -> Optional[float]:
         return float(np.percentile(self.latencies, q)) if self.latencies else None
@@ -170,6 +171,7 @@ class Report:
             "tflops_effective": self.flops_done / self.window / 1e12,
             "by_kind": self.by_kind, "launches": self.launches, "peak_admitted_gb": self.peak_bytes / 1e9,
             "run_s": self.run_s,
+            "host_s": self.host_s,
             "stream_busy_s": self.stream_busy_s,
             "stream_busy_frac": {k: v / self.run_s for k, v in self.stream_busy_s.items()} if self.run_s else {},
         }
@@ -203,6 +205,7 @@ class Server:
         rejected = 0
         nxt = 0
         launches = {FP64: 0, SPLIT: 0}
+        host = {"admit": 0.0, "launch": 0.0, "complete": 0.0}
         t0 = self.clock()
         now = 0.0
         while True:
@@ -223,8 +226,10 @@ class Server:
                     r = queue[i]
                     if in_use + r.nbytes <= self.budget:
                         del queue[i]
+                        ta = self.clock()
                         self.ex.admit(r)
                         r.admitted = self.clock() - t0
+                        host["admit"] += r.admitted + t0 - ta
                         in_use += r.nbytes
                         peak = max(peak, in_use)
                         ready[r.kind].append(r)
@@ -241,6 +246,7 @@ class Server:
                     for r in group:
                         r.dispatched = tnow
                     running[kind].append(Launch(kind, group, self.ex.launch(kind, group)))
+                    host["launch"] += self.clock() - t0 - tnow
                     launches[kind] += 1
             # completions (launches on one stream finish in order)
             progressed = False
@@ -252,6 +258,7 @@ class Server:
                         r.done = tdone
                         self.ex.release(r)
                         in_use -= r.nbytes
+                    host["complete"] += self.clock() - t0 - tdone
                     progressed = True
             busy = any(running.values()) or any(ready.values())
             if not open_ and (not drain or not busy):
@@ -272,7 +279,7 @@ class Server:
         rep = Report(window=window, offered=len(arrived), completed=len(done_in), rejected=rejected,
                      backlog=sum(1 for r in arrived if r.done is None or r.done > window) - rejected,
                      latencies=[r.latency for r in done_in], flops_done=sum(r.flops for r in done_in),
-                     launches=launches, peak_bytes=peak, run_s=run_s,
+                     launches=launches, peak_bytes=peak, run_s=run_s, host_s=host,
                      stream_busy_s=self.ex.busy_seconds() if hasattr(self.ex, "busy_seconds") else {})
         for kind in (FP64, SPLIT):
             ks = [r for r in done_in if r.kind == kind]
@@ -302,6 +309,7 @@ class GpuExecutor:
         self.plans: Dict[str, object] = {}
         self.results: Dict[int, object] = {}
         self.marks: Dict[str, list] = {FP64: [], SPLIT: []}  # (start, end) timing events per launch
+        self.gen = torch.Generator(device="cuda")
 
     def plan(self, name: str):
         if name == "classical":
@@ -311,19 +319,30 @@ class GpuExecutor:
         return self.plans[name]
 
     def operands(self, r: Request):
-        torch, rt = self.torch, self.rt
+        """A, B, C of a request in one device allocation (column-major views, each starting on
+        256 bytes), filled from the request's seed with few calls: at thousands of requests
+        per second the host side of admission is part of the loop's budget."""
+        torch = self.torch
         m, n, k = r.shape
-        g = torch.Generator(device="cuda").manual_seed(self.seed * 1000003 + r.rid)
+        g = self.gen
+        g.manual_seed(self.seed * 1000003 + r.rid)
+        el = 8 if r.kind == FP64 else 4
+        align = 256 // el
+        pad = lambda x: -(-x // align) * align  # noqa: E731
+        oa, ob = 0, pad(m * k)
+        nab = ob + pad(k * n)
+        dt = torch.float64 if r.kind == FP64 else torch.float32
+        ab = torch.empty(nab, dtype=dt, device="cuda")
         if r.kind == FP64:
-            A = rt.colmajor(m, k, device="cuda").uniform_(-1, 1, generator=g)
-            B = rt.colmajor(k, n, device="cuda").uniform_(-1, 1, generator=g)
+            ab.uniform_(-1, 1, generator=g)
         else:
-            A = rt.colmajor(m, k, dtype=torch.float32, device="cuda").normal_(generator=g)
-            e = torch.empty((k, n), device="cuda").uniform_(-10, 10, generator=g)
-            s = torch.empty((k, n), device="cuda").uniform_(-1, 1, generator=g).sign()
-            B = rt.colmajor(k, n, dtype=torch.float32, device="cuda").copy_(s * torch.exp2(e))
-            del e, s
-        C = rt.colmajor(m, n, device="cuda").zero_()
+            ab[:ob].normal_(generator=g)
+            b = ab[ob:]
+            b.uniform_(-20, 20, generator=g)  # sign * 2^U(-10, 10): the sign from the draw's sign
+            b.copy_(torch.sign(b) * torch.exp2(b.abs() - 10))
+        A = ab[oa:oa + m * k].view(k, m).t()
+        B = ab[ob:ob + k * n].view(n, k).t()
+        C = torch.zeros((n, m), dtype=torch.float64, device="cuda").t()  # FP64 in both kinds
         return A, B, C
 
     def admit(self, r: Request) -> None:
