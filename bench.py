@@ -33,10 +33,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-# torch's tensors and the library's workspaces from one stream-ordered pool (the device's
-# default pool, which the library keeps mapped): the serving measurement fills 160 GB of a
-# 180 GB device, and two separate pools would each hold freed memory the other then lacks.
-os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "backend:cudaMallocAsync")
 
 ALGS, LEVELS, PACK = ["222", "333"], [1, 1], "abc"
 SHAPES = [(16384, 16384, 16384), (14400, 14400, 480), (4000, 16000, 2000)]
@@ -418,6 +414,71 @@ def serving_2000(rt, torch, dev, window=1.0, rank=0, world=1):
     return out
 
 
+def run_split2d(args, world, rank, local):
+    """--split2d: each of the workload's three GEMMs split 2-D over the ranks (strong scaling:
+    the total work stays the workload's).  A step per shape: gather the A row panel and the B
+    column panel over the process grid (NCCL all-gather), then the local FMM call on this
+    rank's C block.  value = the workload's effective flops / the slowest rank's time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from fmm_gen_b200 import runtime as rt, shard
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        dist.init_process_group("gloo", store=dist.HashStore(), rank=0, world_size=1)
+    dev = torch.device("cuda", local)
+    plan = rt.Plan.from_levels(ALGS, LEVELS)
+    g = torch.Generator(device=dev).manual_seed(2000 + rank)
+    work = []
+    for (m, n, k) in SHAPES:
+        gm = shard.Gemm2D(m, n, k, plan.algebra.dims)
+        b = gm.blk
+        rows, cols = b.rows[1] - b.rows[0], b.cols[1] - b.cols[0]
+        A_own = rt.colmajor(rows, b.a_k[1] - b.a_k[0], device=dev).uniform_(-1, 1, generator=g)
+        B_own = rt.colmajor(b.b_k[1] - b.b_k[0], cols, device=dev).uniform_(-1, 1, generator=g)
+        C_own = rt.colmajor(rows, cols, device=dev).uniform_(-1, 1, generator=g)
+        work.append((gm, A_own, B_own, C_own))
+
+    def local_gemm(A, B, C):
+        rt.fmm_gemm(plan, A, B, C, PACK)
+
+    def step():
+        for gm, A_own, B_own, C_own in work:
+            gm.run(A_own, B_own, C_own, local_gemm)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev if world > 1 else "cpu")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = effective_flops(SHAPES) * args.steps / (ms * 1e-3) / 1e12
+    if rank == 0:
+        pr, pc = shard.process_grid(world)
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "algorithm": "222-1_333-1", "pack_type": PACK,
+                       "parallelism": f"2-D C split over a {pr}x{pc} grid, panels gathered by all-gather"}}),
+              flush=True)
+    dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,6 +487,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the split-BF16 and batch measurements")
+    ap.add_argument("--split2d", action="store_true",
+                    help="split each GEMM 2-D over the ranks (strong scaling) instead of replicas")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -433,6 +496,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.split2d:
+        run_split2d(args, world, rank, local)
         return
 
     import torch
