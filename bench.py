@@ -16,8 +16,10 @@ one call's copies overlap another's compute; `e2e.serial_value` issues them one 
 One JSON line on rank 0.  Under torchrun (N > 1) every rank runs the same workload on
 its own inputs (independent replicas: a single GEMM is not split across GPUs), and the
 value is the sum over ranks divided by the slowest rank's device time.
-`--impl reference` times the CPU restatement of the reference's algorithm (the oracle)
-on the host cores instead, on rank 0 only.
+`--impl reference` times the reference's own generated multithreaded code for this job on
+the host cores instead (oracle/_ref/fmm, built from an fmm-gen checkout by
+oracle/build_ref_fmm.py; the oracle, its CPU restatement, where those libraries are absent),
+on rank 0 only.
 """
 from __future__ import annotations
 
@@ -121,78 +123,152 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
 
 
-REF_PRODUCTS_PER_STEP = 8  # products of the 16384^3 call's FMM core timed per reference step
+REF_PRODUCTS_PER_STEP = 8  # products of the 16384^3 call's FMM core timed per CPU step
 
 
-class OracleWorkload:
-    """The oracle -- the CPU restatement of the reference's generated abc code, OpenMP over
-    the host cores -- on this bench's workload, with every input made (seeded) and every
-    table built before anything is timed.
+class _CpuWorkload:
+    """This bench's workload on the host cores, with every input made (seeded) and every
+    table or library loaded before anything is timed.
 
     One step runs the 14400x14400x480 and 4000x16000x2000 calls whole, and samples the
     16384^3 call: its FMM core (16368 x 16368 x 16380; the fringe strips are 0.2 % of its
     flops) run over REF_PRODUCTS_PER_STEP of its 161 products, a different group each step
     (all 161 after 21 steps), credited that share of the core's 2mnk.  A whole 16384^3 call
-    takes ~35 s on 16 cores; the sample keeps a step near 4 s.  step() returns the credited
-    effective flops and the seconds spent in the oracle calls alone."""
+    takes tens of seconds on 16 cores; the sample keeps a step at a few seconds.  step()
+    returns the credited effective flops and the seconds spent in the timed calls alone."""
+
+    kind = ""
 
     def __init__(self, seed: int = 99):
         import numpy as np
 
-        from fmm_gen_b200 import algebra, runtime
-        from oracle import cpu
+        from fmm_gen_b200 import algebra
 
-        self.cpu = cpu
         plan = algebra.make_plan(ALGS, LEVELS)
-        dims, nterms, rows, cols, coefs = runtime.plan_tables(plan)
-        self.tables = (dims, plan.rank, nterms, rows, cols, coefs)
+        self.plan = plan
         self.R = plan.rank
         rng = np.random.default_rng(seed)
         self.mats = []
         for (m, n, k) in SHAPES:
             A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
             B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
-            C = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+            C = self._c_buffer(m, n)
+            C[:] = rng.uniform(-1, 1, (m, n))
             self.mats.append((A, B, C))
         m, n, k = SHAPES[0]
         self.core = algebra.partition(m, n, k, plan.dims)
         P = REF_PRODUCTS_PER_STEP
         ngroups = (self.R + P - 1) // P
         self.groups = [[(g * P + i) % self.R for i in range(P)] for g in range(ngroups)]
-        self.subsets = [cpu.product_subset(self.tables, grp) for grp in self.groups]
         self.step_no = 0
-        self.cores = cpu.num_threads()
+
+    def _c_buffer(self, m, n):
+        import numpy as np
+
+        return np.zeros((m, n), order="F")
 
     def step(self):
-        cpu, pc = self.cpu, self.core
+        pc = self.core
         secs, flops = 0.0, 0.0
         for (m, n, k), (A, B, C) in zip(SHAPES[1:], self.mats[1:]):
             t0 = time.perf_counter()
-            cpu.fmm(self.tables, PACK, A, B, C)
+            self._whole(A, B, C)
             secs += time.perf_counter() - t0
             flops += 2.0 * m * n * k
         A, B, C = self.mats[0]
-        sub = self.subsets[self.step_no % len(self.subsets)]
+        g = self.step_no % len(self.groups)
         Ac, Bc, Cc = A[:pc.md, :pc.kd], B[:pc.kd, :pc.nd], C[:pc.md, :pc.nd]
         t0 = time.perf_counter()
-        cpu.fmm(sub, PACK, Ac, Bc, Cc)
+        self._sample(g, Ac, Bc, Cc)
         secs += time.perf_counter() - t0
         flops += 2.0 * pc.md * pc.nd * pc.kd * REF_PRODUCTS_PER_STEP / self.R
         self.step_no += 1
         return flops, secs
 
+    def _sample_text(self, steps):
+        return (f"per step 14400x14400x480 and 4000x16000x2000 whole plus {REF_PRODUCTS_PER_STEP} of the 161 "
+                f"products of the 16384^3 call's FMM core (16368x16368x16380), rotating, credited "
+                f"{REF_PRODUCTS_PER_STEP}/161 of its 2mnk; {steps} steps; inputs generated before timing")
+
+
+class ReferenceWorkload(_CpuWorkload):
+    """The reference's own generated multithreaded code (oracle/build_ref_fmm.py: the
+    222-1_333-1 abc job emitted by its generator and compiled with its runtime and
+    -D_PARALLEL_), on every host core the process may use (BLISLAB_IC_NT).  The sample of the
+    16384^3 call runs one of the job's 8-product libraries: the same generated code for those
+    products.  C is laid out as the reference's driver allocates it (32-byte aligned)."""
+
+    kind = "reference"
+
+    def __init__(self, seed: int = 99):
+        from oracle import build_ref_fmm, cpu
+
+        self.cpu = cpu
+        paths = build_ref_fmm.library_paths()
+        self.cores = len(os.sched_getaffinity(0))
+        cpu.set_ref_threads(self.cores)
+        self.full = cpu.RefFMMLib(paths["full"])
+        self.libs = [cpu.RefFMMLib(p) for p in paths["groups"]]
+        super().__init__(seed)
+        assert len(self.libs) == len(self.groups)
+
+    def _c_buffer(self, m, n):
+        return self.cpu.aligned_colmajor(m, n)
+
+    def _whole(self, A, B, C):
+        self.full(A, B, C)
+
+    def _sample(self, g, A, B, C):
+        self.libs[g](A, B, C)
+
     def describe(self, steps):
-        return (f"oracle/fmm_oracle.c (the reference's abc arithmetic) on {self.cores} host threads; per step "
-                f"14400x14400x480 and 4000x16000x2000 whole plus {REF_PRODUCTS_PER_STEP} of the 161 products of "
-                f"the 16384^3 call's FMM core (16368x16368x16380), rotating, credited {REF_PRODUCTS_PER_STEP}/161 "
-                f"of its 2mnk; {steps} steps; inputs generated before timing")
+        return (f"the reference's generated 222-1_333-1 abc code (its generator + runtime, -D_PARALLEL_, "
+                f"oracle/_ref/fmm) on {self.cores} host threads; " + self._sample_text(steps))
+
+
+class OracleWorkload(_CpuWorkload):
+    """The oracle -- the CPU restatement of the reference's generated abc code, OpenMP over
+    the host cores -- where the reference's own libraries were not built."""
+
+    kind = "port"
+
+    def __init__(self, seed: int = 99):
+        from fmm_gen_b200 import runtime
+        from oracle import cpu
+
+        self.cpu = cpu
+        super().__init__(seed)
+        dims, nterms, rows, cols, coefs = runtime.plan_tables(self.plan)
+        self.tables = (dims, self.R, nterms, rows, cols, coefs)
+        self.subsets = [cpu.product_subset(self.tables, grp) for grp in self.groups]
+        self.cores = cpu.num_threads()
+
+    def _whole(self, A, B, C):
+        self.cpu.fmm(self.tables, PACK, A, B, C)
+
+    def _sample(self, g, A, B, C):
+        self.cpu.fmm(self.subsets[g], PACK, A, B, C)
+
+    def describe(self, steps):
+        return (f"oracle/fmm_oracle.c (the reference's abc arithmetic) on {self.cores} host threads; "
+                + self._sample_text(steps))
+
+
+def cpu_workload():
+    """The reference's own libraries where they were built, else the oracle port."""
+    from oracle import build_ref_fmm
+
+    paths = build_ref_fmm.library_paths()
+    if all(os.path.exists(p) for p in [paths["full"]] + paths["groups"]):
+        return ReferenceWorkload()
+    return OracleWorkload()
 
 
 def run_reference(args, rank):
-    """--impl reference: the CPU restatement of the reference's algorithm, timed on the host."""
+    """--impl reference: the reference's own code for the path (or the oracle), timed on the host."""
     if rank != 0:
         return
-    wl = OracleWorkload()
+    wl = cpu_workload()
     for _ in range(args.warmup):
         wl.step()
     flops, secs = 0.0, 0.0
@@ -209,7 +285,7 @@ def run_reference(args, rank):
         "config": {"workload": WORKLOAD, "algorithm": "222-1_333-1", "pack_type": PACK,
                    "shapes": [list(s) for s in SHAPES], "inputs": "A,B,C ~ U(-1,1), seeded",
                    "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": wl.cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": wl.cores, "kind": wl.kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -685,14 +761,14 @@ def main():
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        wl = OracleWorkload()
+        wl = cpu_workload()
         wl.step()  # warm-up
         cf, cs = 0.0, 0.0
         for _ in range(3):
             f, t = wl.step()
             cf += f
             cs += t
-        cpu_baseline = {"value": cf / cs / 1e12, "unit": UNIT, "cores": wl.cores, "kind": "port",
+        cpu_baseline = {"value": cf / cs / 1e12, "unit": UNIT, "cores": wl.cores, "kind": wl.kind,
                         "sample": wl.describe(3) + f", {cs:.1f} s"}
         del wl
 

@@ -1,6 +1,7 @@
 """ORACLE — test infrastructure only.  ctypes wrapper of liboracle.so (fmm_oracle.c),
-the bit-exact CPU restatement of fmm-gen's arithmetic, and of the reference's own
-classical runtime when it was compiled into _ref/ (Makefile target `ref`).
+the bit-exact CPU restatement of fmm-gen's arithmetic, of the reference's own classical
+runtime when it was compiled into _ref/ (Makefile target `ref`), and of the reference's
+own generated FMM libraries when build_ref_fmm.py compiled them into _ref/fmm/.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use it.
 """
@@ -19,6 +20,10 @@ PACKS = {"abc": 0, "ab": 1, "naive": 2}
 
 _lib = None
 _ref = None
+# The reference's libraries resolve their own symbols first: the product library is loaded
+# RTLD_GLOBAL and exports the same drop-in names (bl_dgemm, bl_dynamic_peeling, ...), which
+# would otherwise take the reference's internal calls (its fringe peeling among them).
+_REF_MODE = ctypes.RTLD_LOCAL | getattr(os, "RTLD_DEEPBIND", 0)
 
 
 def build(ref: bool = False) -> None:
@@ -46,7 +51,7 @@ def load_ref():
     """The reference's classical runtime (bl_dgemm), or None when it was not built."""
     global _ref
     if _ref is None and os.path.exists(REF_LIB):
-        L = ctypes.CDLL(REF_LIB)
+        L = ctypes.CDLL(REF_LIB, mode=_REF_MODE)
         L.bl_dgemm.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_int] * 3
         L.bl_dgemm.restype = None
         _ref = L
@@ -137,3 +142,65 @@ def ref_bl_dgemm(A, B, C) -> bool:
 
 def num_threads() -> int:
     return int(load().oracle_num_threads())
+
+
+# ---------------------------------------------------------------------------------------
+# The reference's generated multithreaded FMM libraries (built by build_ref_fmm.py)
+# ---------------------------------------------------------------------------------------
+_ref_threads = None
+
+
+def aligned_colmajor(m: int, n: int, ld_multiple: int = 8) -> np.ndarray:
+    """A zeroed m x n column-major view laid out as the reference's driver allocates C
+    (meta/misc_gen.py test driver: ldc = ceil(m/8)*8, n+4 columns, 32-byte aligned base);
+    the generated micro-kernels store C with aligned AVX moves."""
+    ld = max(((m - 1) // ld_multiple + 1) * ld_multiple, ld_multiple)
+    buf = np.zeros(ld * (n + 4) + 8)
+    off = (-buf.ctypes.data % 32) // 8
+    flat = buf[off:off + ld * (n + 4)]
+    return flat[: ld * n].reshape(n, ld).T[:m, :]
+
+
+def set_ref_threads(nt: int) -> None:
+    """Threads of the reference libraries (their BLISLAB_IC_NT).  Fixed once per process:
+    each library sizes its packing pool on its first call (bl_malloc_packing_pool,
+    common/dgemm/bl_dgemm_util.c:375-394)."""
+    global _ref_threads
+    if _ref_threads is not None and _ref_threads != nt:
+        raise RuntimeError("the reference libraries' thread count is fixed once per process")
+    _ref_threads = nt
+    os.environ["BLISLAB_IC_NT"] = str(nt)
+
+
+class RefFMMLib:
+    """One generated reference library: bl_dgemm_strassen_abc(m, n, k, A, lda, B, ldb, C, ldc),
+    C += A*B with the reference's packing, AVX micro-kernels and fringe peeling."""
+
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.lib = ctypes.CDLL(path, mode=_REF_MODE)
+        f = self.lib.bl_dgemm_strassen_abc
+        f.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_int] * 3
+        f.restype = None
+        self.fn = f
+
+    def __call__(self, A, B, C) -> None:
+        if _ref_threads is None:
+            raise RuntimeError("call set_ref_threads() first")
+        m, k = A.shape
+        n = B.shape[1]
+        if C.shape != (m, n) or B.shape[0] != k:
+            raise ValueError("shape mismatch")
+        ldc = _ld(C)
+        if C.ctypes.data % 32 or ldc % 8:
+            raise ValueError("C must be 32-byte aligned with a leading dimension that is a multiple of 8 "
+                             "(aligned_colmajor)")
+        if m == 0 or n == 0 or k == 0:
+            return
+        self.fn(m, n, k, _p(A), _ld(A), _p(B), _ld(B), _p(C), ldc)
+
+
+def ref_fmm_dir() -> str:
+    return os.path.join(HERE, "_ref", "fmm")

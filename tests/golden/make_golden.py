@@ -175,8 +175,29 @@ def _fix_asm_operands(path):
         fh.write("\n".join(lines))
 
 
-def build_job(mods, algs, levels, pack, work):
+def _product_subset(gen_mod, products):
+    """Restrict the generator's composed [U,V,W] to the product columns `products` (in that
+    order) while a subset library is emitted: every kept product's code is the one the full
+    generator writes for it, the products are renumbered 0..len-1."""
+    full = gen_mod.generateCoeffs
+
+    def subset(coeffs_mix):
+        return [[[row[r] for r in products] for row in mat] for mat in full(coeffs_mix)]
+
+    gen_mod.generateCoeffs = subset
+    return full
+
+
+def build_job(mods, algs, levels, pack, work, products=None, extra_cflags=(), out=None, compile_now=True):
+    """Emit the reference's C for one job with its own generator and compile it (with the
+    reference runtime) into a shared library; `products` keeps only those products of the
+    composed algorithm (abc only), `out` names the library (default: under `work`); with
+    compile_now=False the gcc command is returned instead of run."""
+    if products is not None and pack != "abc":
+        raise ValueError("product subsets are emitted for the abc pack type only")
     job = job_name(algs, levels) + "_" + pack
+    if products is not None:
+        job += "_p" + "-".join(str(r) for r in products[:1]) + f"x{len(products)}"
     d = os.path.join(work, job)
     for sub in ("dgemm", "kernels", "include"):
         os.makedirs(os.path.join(d, sub), exist_ok=True)
@@ -189,7 +210,13 @@ def build_job(mods, algs, levels, pack, work):
         if pack == "abc":
             mk = f"./kernels/bl_kernel_{job}.c"
             hd = f"./include/bl_kernel_{job}.h"
-            mods["abc_gen_mix"].gen_abc_fmm(files, dims, levels, out_c, mk, hd)
+            gen = mods["abc_gen_mix"]
+            full = _product_subset(gen, products) if products is not None else None
+            try:
+                gen.gen_abc_fmm(files, dims, levels, out_c, mk, hd)
+            finally:
+                if full is not None:
+                    gen.generateCoeffs = full
             srcs.append(os.path.join(d, mk))
         elif pack == "ab":
             mods["ab_gen_mix"].gen_ab_fmm(files, dims, levels, out_c)
@@ -200,12 +227,14 @@ def build_job(mods, algs, levels, pack, work):
     for s in srcs:
         _fix_asm_operands(s)
     common = os.path.join(REF, "common")
-    lib = os.path.join(d, f"lib{job}.so")
-    cmd = [GCC] + CFLAGS + ["-I", os.path.join(d, "include"), "-I", os.path.join(common, "include"), "-o", lib] + srcs + [
+    lib = out or os.path.join(d, f"lib{job}.so")
+    cmd = [GCC] + CFLAGS + list(extra_cflags) + ["-I", os.path.join(d, "include"), "-I", os.path.join(common, "include"), "-o", lib] + srcs + [
         os.path.join(common, "dgemm", "my_dgemm.c"), os.path.join(common, "dgemm", "bl_dgemm_util.c"),
         os.path.join(common, "kernels", "bl_dgemm_asm_8x4.c"),
         os.path.join(common, "kernels", "bl_dgemm_asm_8x4_mulstrassen.c"),
         os.path.join(os.path.dirname(HERE), "..", "oracle", "ref_blas_stub.c")]
+    if not compile_now:
+        return cmd
     subprocess.run(cmd, check=True)
     return lib
 
