@@ -32,6 +32,7 @@ tests drive the same loop with a simulated executor on the CPU.
 """
 from __future__ import annotations
 
+import bisect
 import math
 import time
 from collections import deque
@@ -136,6 +137,71 @@ def poisson_requests(mix: Mix, window: float, seed: int = 0,
     return out
 
 
+class FreeList:
+    """First-fit placement in one address range [0, size): an address-ordered list of free
+    (offset, length) runs, neighbours merged on release.  Offsets and lengths are multiples of
+    `align`.  alloc() returns None when no run is long enough (the caller waits)."""
+
+    def __init__(self, size: int, align: int = 256):
+        self.align = align
+        self.size = size - size % align
+        self.runs: List[Tuple[int, int]] = [(0, self.size)] if self.size else []
+        self.used = 0
+
+    def rounded(self, nbytes: int) -> int:
+        return -(-max(nbytes, 1) // self.align) * self.align
+
+    def alloc(self, nbytes: int) -> Optional[int]:
+        n = self.rounded(nbytes)
+        for i, (off, ln) in enumerate(self.runs):
+            if ln >= n:
+                if ln == n:
+                    del self.runs[i]
+                else:
+                    self.runs[i] = (off + n, ln - n)
+                self.used += n
+                return off
+        return None
+
+    def release(self, off: int, nbytes: int) -> None:
+        n = self.rounded(nbytes)
+        i = bisect.bisect_left(self.runs, (off, 0))
+        if (i < len(self.runs) and self.runs[i][0] < off + n) or (i > 0 and sum(self.runs[i - 1]) > off):
+            raise ValueError("release of a range that is (partly) free")
+        self.used -= n
+        if i > 0 and sum(self.runs[i - 1]) == off:  # merge with the run before
+            off, n = self.runs[i - 1][0], self.runs[i - 1][1] + n
+            i -= 1
+            del self.runs[i]
+        if i < len(self.runs) and self.runs[i][0] == off + n:  # ... and the run after
+            n += self.runs[i][1]
+            del self.runs[i]
+        self.runs.insert(i, (off, n))
+
+    def largest(self) -> int:
+        return max((ln for _, ln in self.runs), default=0)
+
+
+class DeviceArena:
+    """Request operands carved out of one device allocation made up front, so that the loop
+    calls no allocator while it runs (a cudaMalloc of a large block costs the single host
+    thread about a millisecond, a cudaFree waits for the device).  A range returns to the
+    free list only after the launch that used it has completed, so any stream may reuse it."""
+
+    def __init__(self, nbytes: int, align: int = 256):
+        import torch
+
+        self.free = FreeList(nbytes, align)
+        self.buf = torch.empty(self.free.size, dtype=torch.uint8, device="cuda")
+
+    def alloc(self, nbytes: int):
+        off = self.free.alloc(nbytes)
+        return None if off is None else (off, self.buf[off:off + nbytes])
+
+    def release(self, off: int, nbytes: int) -> None:
+        self.free.release(off, nbytes)
+
+
 class Launch:
     """Requests dispatched together, and how to tell that they finished."""
 
@@ -158,6 +224,7 @@ class Report:
     run_s: float = 0.0            # the loop's duration (window plus the drain of admitted work)
     stream_busy_s: Dict[str, float] = field(default_factory=dict)  # per stream: device time of its launches
     host_s: Dict[str, float] = field(default_factory=dict)  # host time in admission, launches, completions
+    declined: int = 0             # admissions the executor declined (no room for the operands yet)
 
     def percentile(self, q: float) -> Optional[float]:
         return float(np.percentile(self.latencies, q)) if self.latencies else None
@@ -172,13 +239,15 @@ class Report:
             "by_kind": self.by_kind, "launches": self.launches, "peak_admitted_gb": self.peak_bytes / 1e9,
             "run_s": self.run_s,
             "host_s": self.host_s,
+            "declined": self.declined,
             "stream_busy_s": self.stream_busy_s,
             "stream_busy_frac": {k: v / self.run_s for k, v in self.stream_busy_s.items()} if self.run_s else {},
         }
 
 
 class Server:
-    """The request loop.  `executor` provides admit(req) (bring operands to the device),
+    """The request loop.  `executor` provides admit(req) (bring operands to the device; False
+    when there is no room for them yet, and the request waits as if the budget were full),
     launch(kind, reqs) -> token, done(token) -> bool, release(req) and sync()."""
 
     def __init__(self, executor, budget_bytes: float = 160e9, max_queue: int = 4096, max_batch: int = 512,
@@ -202,10 +271,11 @@ class Server:
         ready: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
         running: Dict[str, deque] = {FP64: deque(), SPLIT: deque()}
         in_use = peak = 0
-        rejected = 0
+        rejected = declined = 0
         nxt = 0
         launches = {FP64: 0, SPLIT: 0}
         host = {"admit": 0.0, "launch": 0.0, "complete": 0.0}
+        can_hold = getattr(self.ex, "can_hold", lambda r: True)  # could it ever be placed?
         t0 = self.clock()
         now = 0.0
         while True:
@@ -214,7 +284,8 @@ class Server:
             if open_:
                 # arrivals up to now
                 while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                    if len(queue) >= self.max_queue or reqs[nxt].nbytes > self.budget:
+                    if (len(queue) >= self.max_queue or reqs[nxt].nbytes > self.budget
+                            or not can_hold(reqs[nxt])):
                         rejected += 1
                     else:
                         queue.append(reqs[nxt])
@@ -225,15 +296,18 @@ class Server:
                 while i < len(queue) and i < self.scan:
                     r = queue[i]
                     if in_use + r.nbytes <= self.budget:
-                        del queue[i]
                         ta = self.clock()
-                        self.ex.admit(r)
-                        r.admitted = self.clock() - t0
-                        host["admit"] += r.admitted + t0 - ta
-                        in_use += r.nbytes
-                        peak = max(peak, in_use)
-                        ready[r.kind].append(r)
-                        continue
+                        placed = self.ex.admit(r) is not False  # False: no room for its operands yet
+                        if placed:
+                            del queue[i]
+                            r.admitted = self.clock() - t0
+                            host["admit"] += r.admitted + t0 - ta
+                            in_use += r.nbytes
+                            peak = max(peak, in_use)
+                            ready[r.kind].append(r)
+                            continue
+                        host["admit"] += self.clock() - ta
+                        declined += 1
                     if not self.backfill or now - queue[0].arrival > self.head_wait:
                         break
                     i += 1
@@ -279,7 +353,7 @@ class Server:
         rep = Report(window=window, offered=len(arrived), completed=len(done_in), rejected=rejected,
                      backlog=sum(1 for r in arrived if r.done is None or r.done > window) - rejected,
                      latencies=[r.latency for r in done_in], flops_done=sum(r.flops for r in done_in),
-                     launches=launches, peak_bytes=peak, run_s=run_s, host_s=host,
+                     launches=launches, peak_bytes=peak, run_s=run_s, host_s=host, declined=declined,
                      stream_busy_s=self.ex.busy_seconds() if hasattr(self.ex, "busy_seconds") else {})
         for kind in (FP64, SPLIT):
             ks = [r for r in done_in if r.kind == kind]
@@ -298,13 +372,17 @@ class GpuExecutor:
     2^-10..2^10 with random sign for split-BF16; C = 0), so a request can be re-run alone
     with the same inputs; keep=True keeps every result for such comparisons."""
 
-    def __init__(self, seed: int = 0, keep: bool = False):
+    def __init__(self, seed: int = 0, keep: bool = False, arena_bytes: int = 0):
         import torch
 
         from . import runtime as rt
 
         self.torch, self.rt = torch, rt
         self.seed, self.keep = seed, keep
+        # operands from one up-front allocation (DeviceArena) when arena_bytes > 0, else from
+        # torch's caching allocator
+        self.arena = DeviceArena(int(arena_bytes)) if arena_bytes else None
+        self.blocks: Dict[int, Tuple[int, int]] = {}  # rid -> (offset, bytes) in the arena
         self.streams = {FP64: torch.cuda.Stream(), SPLIT: torch.cuda.Stream()}
         self.plans: Dict[str, object] = {}
         self.results: Dict[int, object] = {}
@@ -321,33 +399,52 @@ class GpuExecutor:
     def operands(self, r: Request):
         """A, B, C of a request in one device allocation (column-major views, each starting on
         256 bytes), filled from the request's seed with few calls: at thousands of requests
-        per second the host side of admission is part of the loop's budget."""
+        per second the host side of admission is part of the loop's budget.  None when the
+        arena has no room for them yet."""
         torch = self.torch
         m, n, k = r.shape
+        el = 8 if r.kind == FP64 else 4
+        pad = lambda x: -(-x // 256) * 256  # noqa: E731  (bytes)
+        ob = pad(el * m * k)
+        oc = ob + pad(el * k * n)
+        total = self.operand_bytes(r)
+        if self.arena is not None:
+            got = self.arena.alloc(total)
+            if got is None:
+                return None
+            self.blocks[r.rid] = (got[0], total)
+            buf = got[1]
+        else:
+            buf = torch.empty(total, dtype=torch.uint8, device="cuda")
         g = self.gen
         g.manual_seed(self.seed * 1000003 + r.rid)
-        el = 8 if r.kind == FP64 else 4
-        align = 256 // el
-        pad = lambda x: -(-x // align) * align  # noqa: E731
-        oa, ob = 0, pad(m * k)
-        nab = ob + pad(k * n)
         dt = torch.float64 if r.kind == FP64 else torch.float32
-        ab = torch.empty(nab, dtype=dt, device="cuda")
+        ab = buf[:oc].view(dt)
         if r.kind == FP64:
             ab.uniform_(-1, 1, generator=g)
         else:
-            ab[:ob].normal_(generator=g)
-            b = ab[ob:]
+            ab[:ob // el].normal_(generator=g)
+            b = ab[ob // el:]
             b.uniform_(-20, 20, generator=g)  # sign * 2^U(-10, 10): the sign from the draw's sign
             b.copy_(torch.sign(b) * torch.exp2(b.abs() - 10))
-        A = ab[oa:oa + m * k].view(k, m).t()
-        B = ab[ob:ob + k * n].view(n, k).t()
-        C = torch.zeros((n, m), dtype=torch.float64, device="cuda").t()  # FP64 in both kinds
+        A = ab[:m * k].view(k, m).t()
+        B = ab[ob // el:ob // el + k * n].view(n, k).t()
+        C = buf[oc:total].view(torch.float64).zero_().view(n, m).t()  # FP64 in both kinds
         return A, B, C
 
-    def admit(self, r: Request) -> None:
+    def operand_bytes(self, r: Request) -> int:
+        m, n, k = r.shape
+        el = 8 if r.kind == FP64 else 4
+        pad = lambda x: -(-x // 256) * 256  # noqa: E731
+        return pad(el * m * k) + pad(el * k * n) + 8 * m * n
+
+    def can_hold(self, r: Request) -> bool:
+        return self.arena is None or self.arena.free.rounded(self.operand_bytes(r)) <= self.arena.free.size
+
+    def admit(self, r: Request):
         with self.torch.cuda.stream(self.streams[r.kind]):
             r.handle = self.operands(r)
+        return r.handle is not None
 
     def launch(self, kind: str, reqs: List[Request]):
         torch, rt = self.torch, self.rt
@@ -378,13 +475,43 @@ class GpuExecutor:
         if self.keep:
             self.results[r.rid] = r.handle[2].cpu()
         r.handle = None
+        self.free_operands(r.rid)  # the launch that used them has completed
+
+    def free_operands(self, rid: int) -> None:
+        """Return a request's arena range (no-op without an arena: torch frees the tensors)."""
+        blk = self.blocks.pop(rid, None)
+        if blk is not None:
+            self.arena.release(*blk)
 
     def sync(self) -> None:
         self.torch.cuda.synchronize()
 
+    def warm(self, requests: Sequence[Request]) -> None:
+        """First-use costs outside any timed window: every (kind, algorithm) of `requests` runs
+        once alone (its plan's tables are uploaded, the workspace pool grows to the largest
+        of them), and one FP64 request once through a batch launch."""
+        largest: Dict[Tuple[str, str], Request] = {}
+        for r in requests:
+            key = (r.kind, r.algorithm)
+            if key not in largest or r.flops > largest[key].flops:
+                largest[key] = r
+        for r in largest.values():
+            self.run_alone(r)
+        fp = next((r for r in requests if r.kind == FP64), None)
+        if fp is not None:
+            ops = self.operands(fp)
+            if ops is not None:
+                A, B, C = ops
+                self.rt.batch_submit([self.plan(fp.algorithm)], [A], [B], [C], stream=self.streams[FP64])
+                self.torch.cuda.synchronize()
+                self.free_operands(fp.rid)
+
     def run_alone(self, r: Request):
         """The request by itself (same inputs, same algorithm), for comparison."""
-        A, B, C = self.operands(r)
+        ops = self.operands(r)
+        if ops is None:
+            raise RuntimeError("no room in the arena for the request's operands")
+        A, B, C = ops
         if r.kind == FP64:
             p = self.plan(r.algorithm)
             if p is None:
@@ -394,7 +521,9 @@ class GpuExecutor:
         else:
             self.rt.split_gemm(self.plan(r.algorithm), A, B, C)
         self.torch.cuda.synchronize()
-        return C.cpu()
+        out = C.cpu()
+        self.free_operands(r.rid)
+        return out
 
 
 def shard_requests(requests: Sequence[Request], world: int, model: Optional[tuner.B200Model] = None) -> List[List[Request]]:

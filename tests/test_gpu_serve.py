@@ -2,7 +2,9 @@
 FMM and classical) and split-BF16 requests under a small HBM budget, so requests queue,
 batch and overlap.  Every result must be bit-identical to the same request run alone
 (same inputs, same algorithm), and correct against an FP64 reference: relative
-Frobenius error <= 1e-13 for FP64 requests, <= 1e-6 for split-BF16 ones."""
+Frobenius error <= 1e-13 for FP64 requests, <= 1e-6 for split-BF16 ones.  Run with operands
+from torch's caching allocator and from the executor's arena (smaller than the budget, so some
+admissions are declined until a range frees up)."""
 import pytest
 
 torch = pytest.importorskip("torch")
@@ -20,7 +22,8 @@ def _lib():
     rt.load_library()
 
 
-def test_results_are_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("arena_bytes", [0, 0.5e9], ids=["torch_allocator", "arena"])
+def test_results_are_the_same_alone_and_in_the_mix(arena_bytes):
     mix = serve.Mix(rate=600.0, f_rank_k=0.1, f_split=0.2, lo=200, hi=1500, rank_k_shape=(3000, 3000, 256),
                     split_shape=(1024, 1024, 1024), split_algorithm="222-1")
     reqs = serve.poisson_requests(mix, 0.15, seed=11)
@@ -28,7 +31,7 @@ def test_results_are_the_same_alone_and_in_the_mix():
     for r in reqs[:6]:
         if r.kind == serve.FP64:
             r.algorithm = "222-1"
-    ex = serve.GpuExecutor(seed=5, keep=True)
+    ex = serve.GpuExecutor(seed=5, keep=True, arena_bytes=arena_bytes)
     for kind in (serve.FP64, serve.SPLIT):  # first-use costs (plans, kernels) outside the loop
         ex.run_alone(next(r for r in reqs if r.kind == kind))
     # all arrivals come in the first 0.15 s; the window is long enough for every request
@@ -44,5 +47,7 @@ def test_results_are_the_same_alone_and_in_the_mix():
     for r in [q for q in done if q.kind == serve.SPLIT][:3] + [q for q in done if q.kind == serve.FP64][:5]:
         A, B, C = ex.operands(r)
         ref = (A.double() @ B.double()).cpu()
+        torch.cuda.synchronize()
+        ex.free_operands(r.rid)
         err = ((ex.results[r.rid] - ref).norm() / ref.norm()).item()
         assert err <= (1e-6 if r.kind == serve.SPLIT else 1e-13), (r.kind, r.shape, err)

@@ -158,3 +158,87 @@ def test_backfill_stops_when_the_waiting_request_has_waited_long_enough():
     assert 1 in ex.admitted
     pos = ex.admitted.index(1)
     assert pos < len(ex.admitted) - 1  # admitted while small requests were still arriving
+
+
+def test_free_list_places_first_fit_and_merges_neighbours():
+    fl = serve.FreeList(10 * 256, align=256)
+    a = fl.alloc(256)
+    b = fl.alloc(300)            # rounded up to 512
+    c = fl.alloc(256)
+    assert (a, b, c) == (0, 256, 768) and fl.used == 1024
+    assert fl.alloc(7 * 256) is None  # 6 blocks left
+    fl.release(b, 300)
+    assert fl.alloc(512) == 256  # first fit reuses the hole
+    fl.release(256, 512)
+    fl.release(a, 256)
+    fl.release(c, 256)           # all three merge back with the tail
+    assert fl.runs == [(0, 10 * 256)] and fl.used == 0
+    with pytest.raises(ValueError):
+        fl.release(0, 256)       # already free
+
+
+def test_free_list_random_sequence_matches_a_bitmap():
+    rng = np.random.default_rng(7)
+    size, align = 4096, 16
+    fl = serve.FreeList(size, align)
+    taken = np.zeros(size // align, dtype=bool)
+    live = []
+    for _ in range(3000):
+        if live and rng.random() < 0.45:
+            off, n = live.pop(int(rng.integers(len(live))))
+            fl.release(off, n)
+            taken[off // align:(off + fl.rounded(n)) // align] = False
+        else:
+            n = int(rng.integers(1, 400))
+            off = fl.alloc(n)
+            blocks = fl.rounded(n) // align
+            # first fit: the lowest free run that is long enough
+            want = None
+            run = 0
+            for i, t in enumerate(taken):
+                run = 0 if t else run + 1
+                if run == blocks:
+                    want = (i - blocks + 1) * align
+                    break
+            assert off == want
+            if off is not None:
+                assert not taken[off // align:off // align + blocks].any()
+                taken[off // align:off // align + blocks] = True
+                live.append((off, n))
+        free_runs = sum(ln for _, ln in fl.runs)
+        assert free_runs == size - int(taken.sum()) * align == size - fl.used
+        assert all(fl.runs[i][0] + fl.runs[i][1] < fl.runs[i + 1][0] for i in range(len(fl.runs) - 1))
+
+
+class ArenaSimExecutor(SimExecutor):
+    """The simulated GPU with an operand arena: admission is declined while the arena has no
+    room for the request's operands, whatever the budget says."""
+
+    def __init__(self, clock, arena_bytes):
+        super().__init__(clock)
+        self.fl = serve.FreeList(arena_bytes, 256)
+        self.where = {}
+
+    def admit(self, r):
+        off = self.fl.alloc(r.nbytes)
+        if off is None:
+            return False
+        self.where[r.rid] = off
+        return super().admit(r)
+
+    def release(self, r):
+        self.fl.release(self.where.pop(r.rid), r.nbytes)
+        super().release(r)
+
+
+def test_requests_wait_while_the_executor_declines_them():
+    mix = serve.Mix(rate=400.0, f_rank_k=0.5, f_split=0.0, lo=256, hi=1024)
+    reqs = serve.poisson_requests(mix, 0.3, seed=4)
+    big = max(r.nbytes for r in reqs)
+    clk = SimClock()
+    ex = ArenaSimExecutor(clk, 3 * big)      # room for about three rank-k requests at once
+    rep = serve.Server(ex, budget_bytes=1e15, clock=clk, sleep=clk.sleep).run(reqs, 0.3)
+    assert rep.declined > 0                  # the budget alone would have admitted them
+    assert sorted(ex.released) == sorted(ex.admitted)
+    assert ex.fl.used == 0 and ex.fl.runs == [(0, ex.fl.size)]
+    assert rep.completed + rep.backlog + rep.rejected == rep.offered
