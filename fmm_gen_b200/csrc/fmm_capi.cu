@@ -13,12 +13,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <iterator>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/fmm_b200.h"
@@ -101,6 +103,10 @@ struct DevTables {
   int* cblk = nullptr;
   int* ent_r = nullptr;
   double* ent_w = nullptr;
+  int* cg_desc = nullptr;  // grouped combine tables
+  int* cg_r = nullptr;
+  int* cg_m = nullptr;
+  double* cg_c = nullptr;
   fmm::Prod* prods_ps = nullptr;  // products over pre-summed operands (one A and one B term each)
   fmm::Term* terms_ps = nullptr;
   int* plistA = nullptr;          // products whose A operand is pre-summed, in slot order
@@ -133,6 +139,11 @@ struct fmm_plan {
   std::vector<double> ent_w;
   int n_cblk = 0;
   int n_cterms = 0;  // C terms over all products
+  // The same lists with the blocks in groups that share products (fmm_combine_kernel's
+  // tables: group descriptors, merged entries and their coefficients; see build_combine_groups).
+  std::vector<int> cg_desc, cg_r, cg_m;
+  std::vector<double> cg_c;
+  int n_cgroup = 0;
   // Pre-summed form: each product's A operand is either its single A block (src 0) or
   // slot j of the workspace S (src 1) that holds sum_i U[i,r] A_i; likewise for B / T.
   std::vector<fmm::Prod> prods_ps;
@@ -179,6 +190,18 @@ int upload_tables(fmm_plan* p, DevTables& d) {
   if (!p->ent_r.empty()) {
     FMM_CUDA_TRY(cudaMemcpy(d.ent_r, p->ent_r.data(), sizeof(int) * p->ent_r.size(), cudaMemcpyHostToDevice));
     FMM_CUDA_TRY(cudaMemcpy(d.ent_w, p->ent_w.data(), sizeof(double) * p->ent_w.size(), cudaMemcpyHostToDevice));
+  }
+  {
+    auto up = [](auto** dst, const auto& v) -> cudaError_t {
+      using T = typename std::decay_t<decltype(v)>::value_type;
+      cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.size() ? v.size() : 1));
+      if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+      return e;
+    };
+    FMM_CUDA_TRY(up(&d.cg_desc, p->cg_desc));
+    FMM_CUDA_TRY(up(&d.cg_r, p->cg_r));
+    FMM_CUDA_TRY(up(&d.cg_m, p->cg_m));
+    FMM_CUDA_TRY(up(&d.cg_c, p->cg_c));
   }
   FMM_CUDA_TRY(cudaMalloc(&d.prods_ps, sizeof(fmm::Prod) * p->prods_ps.size()));
   FMM_CUDA_TRY(cudaMalloc(&d.terms_ps, sizeof(fmm::Term) * p->terms_ps.size()));
@@ -325,6 +348,96 @@ int ksplit_tables(const fmm_plan* cp, int base, int S, const fmm::Prod** prods, 
   return FMM_OK;
 }
 
+// Blocks of the C grid in groups of up to fmm::COMBINE_GROUP that share products, for
+// fmm_combine_kernel: greedily merge the two groups whose product sets overlap most (while
+// the merged group fits), up to 64 blocks; beyond that, consecutive blocks.  Then one merged
+// entry per product of a group's union (increasing r) with the mask of the members it
+// updates and their coefficients in member order.
+void build_combine_groups(fmm_plan* p) {
+  const int nb = p->n_cblk;
+  std::vector<std::vector<int>> mem(nb), uni(nb);
+  for (int b = 0; b < nb; ++b) {
+    mem[b] = {b};
+    const int e0 = p->cblk[4 * b + 2], ne = p->cblk[4 * b + 3];
+    uni[b].assign(p->ent_r.begin() + e0, p->ent_r.begin() + e0 + ne);  // increasing r
+  }
+  auto overlap = [](const std::vector<int>& x, const std::vector<int>& y) {
+    size_t i = 0, j = 0;
+    int n = 0;
+    while (i < x.size() && j < y.size()) {
+      if (x[i] == y[j]) ++n, ++i, ++j;
+      else if (x[i] < y[j]) ++i;
+      else ++j;
+    }
+    return n;
+  };
+  if (nb <= 64) {
+    for (;;) {
+      int best = 0, bi = -1, bj = -1;
+      for (int i = 0; i < (int)mem.size(); ++i)
+        for (int j = i + 1; j < (int)mem.size(); ++j) {
+          if ((int)(mem[i].size() + mem[j].size()) > fmm::COMBINE_GROUP) continue;
+          const int ov = overlap(uni[i], uni[j]);
+          if (ov > best) best = ov, bi = i, bj = j;
+        }
+      if (bi < 0) break;
+      mem[bi].insert(mem[bi].end(), mem[bj].begin(), mem[bj].end());
+      std::vector<int> u;
+      std::set_union(uni[bi].begin(), uni[bi].end(), uni[bj].begin(), uni[bj].end(), std::back_inserter(u));
+      uni[bi] = u;
+      mem.erase(mem.begin() + bj);
+      uni.erase(uni.begin() + bj);
+    }
+  } else {
+    std::vector<std::vector<int>> m2, u2;
+    for (int b = 0; b < nb; b += fmm::COMBINE_GROUP) {
+      std::vector<int> g, u;
+      for (int q = b; q < std::min(nb, b + fmm::COMBINE_GROUP); ++q) {
+        g.push_back(q);
+        std::vector<int> t;
+        std::set_union(u.begin(), u.end(), uni[q].begin(), uni[q].end(), std::back_inserter(t));
+        u = t;
+      }
+      m2.push_back(g);
+      u2.push_back(u);
+    }
+    mem = m2;
+    uni = u2;
+  }
+  p->cg_desc.clear();
+  p->cg_r.clear();
+  p->cg_m.clear();
+  p->cg_c.clear();
+  for (size_t g = 0; g < mem.size(); ++g) {
+    const int first = (int)p->cg_r.size(), firstc = (int)p->cg_c.size();
+    std::vector<size_t> pos(mem[g].size(), 0);  // cursor into each member's (increasing r) list
+    for (int r : uni[g]) {
+      int mask = 0;
+      const int k0 = (int)p->cg_c.size();
+      for (size_t q = 0; q < mem[g].size(); ++q) {
+        const int b = mem[g][q];
+        const int e0 = p->cblk[4 * b + 2], ne = p->cblk[4 * b + 3];
+        if (pos[q] < (size_t)ne && p->ent_r[e0 + pos[q]] == r) {
+          mask |= 1 << q;
+          p->cg_c.push_back(p->ent_w[e0 + pos[q]]);
+          ++pos[q];
+        }
+      }
+      p->cg_r.push_back(r);
+      p->cg_m.push_back(mask | (k0 << 8));
+    }
+    p->cg_desc.push_back(first);
+    p->cg_desc.push_back((int)p->cg_r.size() - first);
+    p->cg_desc.push_back((int)mem[g].size());
+    p->cg_desc.push_back(firstc);
+    for (int q = 0; q < fmm::COMBINE_GROUP; ++q) {
+      const int b = q < (int)mem[g].size() ? mem[g][q] : mem[g][0];
+      p->cg_desc.push_back(p->cblk[4 * b] * p->dims[2] + p->cblk[4 * b + 1]);
+    }
+  }
+  p->n_cgroup = (int)mem.size();
+}
+
 int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, const int* cols,
                const double* coefs, fmm_plan** out) {
   if (!dims || !nterms || !rows || !cols || !coefs || !out || rank <= 0) return FMM_E_INVALID;
@@ -393,6 +506,7 @@ int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, 
     }
     ++p->n_cblk;
   }
+  build_combine_groups(p);
   for (int r = 0; r < rank; ++r) {
     const fmm::Prod& pr = p->prods[r];
     fmm::Prod q{};
@@ -744,14 +858,16 @@ int peel(int m, int n, int k, const double* A, long long lda, const double* B, l
 }
 
 // C_l += sum_r W[l,r] * M_r for every C block at once (fmm_combine_kernel); false when the
-// plan is too large for its shared-memory tables (the caller then uses the per-block scatter).
+// plan's grouped tables do not fit the kernel's shared memory (the caller then uses the
+// per-block scatter).
 bool combine_fits(const fmm_plan* plan) {
-  const int nblk = plan->dims[0] * plan->dims[2];
-  return nblk <= fmm::COMBINE_MAX_BLOCKS && plan->n_cterms <= fmm::COMBINE_MAX_TERMS &&
-         fmm::combine_smem_bytes(nblk, plan->n_cterms, plan->rank) <= 200 * 1024;
+  return plan->n_cgroup > 0 &&
+         fmm::combine_group_smem_bytes(plan->n_cgroup, (int)plan->cg_r.size(), (int)plan->cg_c.size()) <= 200 * 1024;
 }
 
 bool combine_configured[kMaxDevices];
+// element positions per thread of the combine (fmm_debug_set FMM_DEBUG_COMBINE_POSITIONS; 0: 1)
+std::atomic<int> g_combine_positions{0};
 
 int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long long ldc, int ms, int ns,
                    const double* M, long long ldm, long long m_stride, cudaStream_t st) {
@@ -760,33 +876,40 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
   {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (!combine_configured[dev]) {
-      FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
+      FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         200 * 1024));
       combine_configured[dev] = true;
     }
   }
-  fmm::CombineArgs ca{};
-  ca.C = C;
-  ca.ldc = ldc;
-  ca.ms = ms;
-  ca.ns = ns;
-  ca.M = M;
-  ca.ldm = ldm;
-  ca.m_stride = m_stride;
-  ca.prods = d.prods;
-  ca.terms = d.terms;
-  ca.nprod = plan->rank;
-  ca.nterms = plan->n_cterms;
-  ca.grid_m = plan->dims[0];
-  ca.grid_n = plan->dims[2];
-  // many C blocks: smaller CTAs, so that more of them (and more loads in flight) fit per SM
-  const int threads = ca.grid_m * ca.grid_n > 16 ? fmm::COMBINE_THREADS / 2 : fmm::COMBINE_THREADS;
-  const size_t smem = fmm::combine_smem_bytes(ca.grid_m * ca.grid_n, ca.nterms, ca.nprod, threads);
-  const long long blocks = ((long long)ms * ns + threads - 1) / threads;
-  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, 148LL * 16));
+  fmm::CombineGroupArgs ga{};
+  ga.C = C;
+  ga.ldc = ldc;
+  ga.ms = ms;
+  ga.ns = ns;
+  ga.M = M;
+  ga.ldm = ldm;
+  ga.m_stride = m_stride;
+  ga.grid_n = plan->dims[2];
+  ga.ngroup = plan->n_cgroup;
+  ga.nent = (int)plan->cg_r.size();
+  ga.ncoef = (int)plan->cg_c.size();
+  ga.gdesc = d.cg_desc;
+  ga.er = d.cg_r;
+  ga.em = d.cg_m;
+  ga.ec = d.cg_c;
+  const int P = g_combine_positions.load() == 2 ? 2 : 1;
+  const size_t smem = fmm::combine_group_smem_bytes(ga.ngroup, ga.nent, ga.ncoef);
+  const long long per = (long long)fmm::COMBINE_G_THREADS * P;
+  const long long blocks = ((long long)ms * ns + per - 1) / per;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(blocks, (long long)sm_count_current() * 8));
   {
     ProfScope pf(K_COMBINE, st);
-    fmm::fmm_combine_kernel<<<grid, threads, smem, st>>>(ca);
+    if (P == 2)
+      fmm::fmm_combine_kernel<2><<<grid, fmm::COMBINE_G_THREADS, smem, st>>>(ga);
+    else
+      fmm::fmm_combine_kernel<1><<<grid, fmm::COMBINE_G_THREADS, smem, st>>>(ga);
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cuda_status(cudaGetLastError());
@@ -1392,6 +1515,10 @@ int fmm_plan_destroy(fmm_plan* plan) {
     cudaFree(d.cblk);
     cudaFree(d.ent_r);
     cudaFree(d.ent_w);
+    cudaFree(d.cg_desc);
+    cudaFree(d.cg_r);
+    cudaFree(d.cg_m);
+    cudaFree(d.cg_c);
     cudaFree(d.prods_ps);
     cudaFree(d.terms_ps);
     cudaFree(d.plistA);
@@ -1542,6 +1669,10 @@ int fmm_debug_set(int what, long long value) {
     case FMM_DEBUG_TICKET_FILL:
       if (value < 0 || value > 255) return FMM_E_INVALID;
       g_ticket_fill = (int)value;
+      return FMM_OK;
+    case FMM_DEBUG_COMBINE_POSITIONS:
+      if (value < 0 || value > 2) return FMM_E_INVALID;
+      g_combine_positions = (int)value;
       return FMM_OK;
     default:
       return FMM_E_INVALID;

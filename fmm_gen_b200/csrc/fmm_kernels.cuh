@@ -1587,117 +1587,6 @@ __global__ void fmm_lincomb_batch_kernel(const LincombTask* tasks) {
   for (long long c = blockIdx.y; c < nchunk; c += gridDim.y) lincomb_body(tk.a, blockIdx.x, c);
 }
 
-// C_l += sum_r W[l, r] * M_r for every C block l of the plan's grid at once: a thread owns
-// one element position, keeps the running value of that position in every C block in
-// shared memory (loaded from C first), and applies the products in order r = 0..R-1 with
-// the same fma sequence as the epilogue's multi-destination update.  Each M_r and each C
-// element cross HBM once: bytes per position 8 (R + 2 * blocks).  The product -> (block,
-// coefficient) table is staged in shared memory once per CTA.
-struct CombineArgs {
-  double* C;
-  long long ldc;
-  int ms, ns;
-  const double* M;
-  long long ldm;
-  long long m_stride;
-  const Prod* prods;
-  const Term* terms;
-  int nprod;
-  int nterms;          // C terms over all products (sum of nc)
-  int grid_m, grid_n;  // C block grid
-};
-
-constexpr int COMBINE_THREADS = 256;  // threads per CTA (128 when the plan has more than 16 C blocks)
-constexpr int COMBINE_MAX_BLOCKS = 64;
-constexpr int COMBINE_MAX_TERMS = 4096;
-constexpr int COMBINE_BATCH = 8;
-constexpr int COMBINE_TERMS = 4;  // C terms of one product updated together (their blocks differ)
-
-__host__ __device__ constexpr size_t combine_smem_bytes(int nblk, int nterms, int nprod, int threads = COMBINE_THREADS) {
-  return sizeof(double) * (size_t)nblk * threads + (sizeof(double) + sizeof(int)) * (size_t)nterms +
-         sizeof(int) * (size_t)(nprod + 1);
-}
-
-__global__ void __launch_bounds__(COMBINE_THREADS) fmm_combine_kernel(const CombineArgs a) {
-  extern __shared__ __align__(16) double cacc[];
-  const int nt = blockDim.x;
-  const int nblk = a.grid_m * a.grid_n;
-  double* tcoef = cacc + (size_t)nblk * nt;
-  int* tblk = reinterpret_cast<int*>(tcoef + a.nterms);
-  int* tfirst = tblk + a.nterms;  // compact C-term ranges per product, nprod + 1 entries
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int r = 0; r < a.nprod; ++r) {
-      tfirst[r] = acc;
-      acc += a.prods[r].nc;
-    }
-    tfirst[a.nprod] = acc;
-  }
-  __syncthreads();
-  for (int r = threadIdx.x; r < a.nprod; r += nt) {
-    const Prod p = a.prods[r];
-    for (int c = 0; c < p.nc; ++c) {
-      const Term t = a.terms[p.c0 + c];
-      tcoef[tfirst[r] + c] = t.coef;
-      tblk[tfirst[r] + c] = t.row * a.grid_n + t.col;
-    }
-  }
-  __syncthreads();
-  const int tid = threadIdx.x;
-  const long long total = (long long)a.ms * a.ns;
-  for (long long e0 = (long long)blockIdx.x * nt; e0 < total; e0 += (long long)gridDim.x * nt) {
-    const long long e = e0 + tid;
-    if (e >= total) continue;
-    const int i = (int)(e % a.ms);
-    const long long j = e / a.ms;
-    // loads in groups of COMBINE_BATCH independent ones, so each thread keeps that many in
-    // flight (a bandwidth-bound pass needs the memory parallelism)
-    for (int b0 = 0; b0 < nblk; b0 += COMBINE_BATCH) {
-      double v[COMBINE_BATCH];
-#pragma unroll
-      for (int q = 0; q < COMBINE_BATCH; ++q) {
-        const int b = b0 + q;
-        v[q] = b < nblk ? a.C[(long long)(b / a.grid_n) * a.ms + i + ((long long)(b % a.grid_n) * a.ns + j) * a.ldc]
-                        : 0.0;
-      }
-#pragma unroll
-      for (int q = 0; q < COMBINE_BATCH; ++q)
-        if (b0 + q < nblk) cacc[(size_t)(b0 + q) * nt + tid] = v[q];
-    }
-    for (int r0 = 0; r0 < a.nprod; r0 += COMBINE_BATCH) {
-      double m[COMBINE_BATCH];
-#pragma unroll
-      for (int q = 0; q < COMBINE_BATCH; ++q)
-        m[q] = r0 + q < a.nprod ? a.M[(long long)(r0 + q) * a.m_stride + i + j * a.ldm] : 0.0;
-#pragma unroll
-      for (int q = 0; q < COMBINE_BATCH; ++q) {
-        const int r = r0 + q;
-        if (r >= a.nprod) break;
-        // a product's C terms name distinct blocks: their values are read together, then
-        // updated and written back, instead of one dependent read-update-write per term
-        for (int c = tfirst[r]; c < tfirst[r + 1]; c += COMBINE_TERMS) {
-          double x[COMBINE_TERMS], w[COMBINE_TERMS];
-          double* px[COMBINE_TERMS];
-#pragma unroll
-          for (int t = 0; t < COMBINE_TERMS; ++t) {
-            const bool ok = c + t < tfirst[r + 1];
-            px[t] = cacc + (size_t)(ok ? tblk[c + t] : 0) * nt + tid;
-            w[t] = ok ? tcoef[c + t] : 0.0;
-            x[t] = ok ? *px[t] : 0.0;
-          }
-#pragma unroll
-          for (int t = 0; t < COMBINE_TERMS; ++t)
-            if (c + t < tfirst[r + 1]) *px[t] = fma(w[t], m[q], x[t]);
-        }
-      }
-    }
-    for (int b = 0; b < nblk; ++b) {
-      const int br = b / a.grid_n, bc = b % a.grid_n;
-      a.C[(long long)br * a.ms + i + ((long long)bc * a.ns + j) * a.ldc] = cacc[(size_t)b * nt + tid];
-    }
-  }
-}
-
 // Column-major copies between pitches, many in one launch (task blockIdx.y): used to give
 // operands with an odd leading dimension the even pitch (16-byte column starts) that
 // tensor-memory-access staging needs.
@@ -1719,6 +1608,122 @@ __device__ __forceinline__ void pitch_copy_body(const PitchCopy& t) {
 
 __global__ void fmm_pitch_copy_kernel(const PitchCopy* tasks) { pitch_copy_body(tasks[blockIdx.y]); }
 __global__ void fmm_pitch_copy1_kernel(const PitchCopy t) { pitch_copy_body(t); }
+
+// C_l += sum_r W[l, r] * M_r for every C block, the blocks in groups of up to COMBINE_GROUP: a
+// thread owns P element positions and walks the groups; for a group it keeps the running values of
+// its member blocks in registers, walks the union of their products in increasing r (one
+// load of M_r per position, COMBINE_G_BATCH loads in flight) and applies M_r to every member
+// whose W[l, r] is nonzero, c_l = fma(W[l, r], M_r, c_l).  Each block still gets exactly the
+// epilogue's fma sequence (products in increasing r), so the result is bit-identical to the
+// direct schedule.  The host groups blocks that share products (greedy by overlap), which
+// cuts the M loads per position from nnz(W) toward R (222-1 x 333-1: 540 -> 299 in 5
+// groups) with no shared-memory read-modify-write.  Tables (shared memory, per CTA):
+//   group g: gdesc[g * GDESC + 0..3] = first entry, #entries, #members, first coefficient;
+//            gdesc[g * GDESC + 4 + q] = block id of member q (row * grid_n + col)
+//   entry e: er[e] = product r, em[e] = member mask | (first coefficient of e) << 8,
+//            the coefficients of its set bits, member order, from ec[first coefficient]
+constexpr int COMBINE_GROUP = 8;
+constexpr int GDESC = 4 + COMBINE_GROUP;
+constexpr int COMBINE_G_THREADS = 256;
+constexpr int COMBINE_G_BATCH = 16;
+
+struct CombineGroupArgs {
+  double* C;
+  long long ldc;
+  int ms, ns;
+  const double* M;
+  long long ldm;
+  long long m_stride;
+  int grid_n;
+  int ngroup, nent, ncoef;
+  const int* gdesc;
+  const int* er;
+  const int* em;
+  const double* ec;
+};
+
+__host__ __device__ constexpr size_t combine_group_smem_bytes(int ngroup, int nent, int ncoef) {
+  return sizeof(double) * (size_t)ncoef + sizeof(int) * (2 * (size_t)nent + (size_t)GDESC * ngroup) + 16;
+}
+
+template <int P>
+__global__ void __launch_bounds__(COMBINE_G_THREADS) fmm_combine_kernel(const CombineGroupArgs a) {
+  extern __shared__ __align__(16) double gtab[];
+  double* sc = gtab;                               // [ncoef]
+  int* sr = reinterpret_cast<int*>(sc + a.ncoef);  // [nent]
+  int* sm = sr + a.nent;                           // [nent]
+  int* sg = sm + a.nent;                           // [GDESC * ngroup]
+  for (int q = threadIdx.x; q < a.ncoef; q += blockDim.x) sc[q] = a.ec[q];
+  for (int q = threadIdx.x; q < a.nent; q += blockDim.x) {
+    sr[q] = a.er[q];
+    sm[q] = a.em[q];
+  }
+  for (int q = threadIdx.x; q < GDESC * a.ngroup; q += blockDim.x) sg[q] = a.gdesc[q];
+  __syncthreads();
+  const int nt = blockDim.x;
+  const long long total = (long long)a.ms * a.ns;
+  for (long long e0 = (long long)blockIdx.x * nt * P; e0 < total; e0 += (long long)gridDim.x * nt * P) {
+    // position p of this thread: e0 + threadIdx.x + p * nt (clamped to the last one, whose
+    // stores then repeat the same values)
+    long long cofs[P], mofs[P];
+    bool live[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const long long e = e0 + threadIdx.x + (long long)p * nt;
+      live[p] = e < total;
+      const long long ee = live[p] ? e : total - 1;
+      const int i = (int)(ee % a.ms);
+      const long long j = ee / a.ms;
+      cofs[p] = i + j * a.ldc;
+      mofs[p] = i + j * a.ldm;
+    }
+    if (!live[0]) continue;
+#pragma unroll 1
+    for (int g = 0; g < a.ngroup; ++g) {
+      const int* gd = sg + g * GDESC;
+      const int ef = gd[0], ne = gd[1], nm = gd[2];
+      double c[COMBINE_GROUP][P];
+      long long cb[COMBINE_GROUP];
+#pragma unroll
+      for (int q = 0; q < COMBINE_GROUP; ++q) {
+        const int b = gd[4 + (q < nm ? q : 0)];
+        cb[q] = (long long)(b / a.grid_n) * a.ms + (long long)(b % a.grid_n) * a.ns * a.ldc;
+#pragma unroll
+        for (int p = 0; p < P; ++p) c[q][p] = q < nm ? a.C[cb[q] + cofs[p]] : 0.0;
+      }
+#pragma unroll 1
+      for (int q0 = 0; q0 < ne; q0 += COMBINE_G_BATCH) {
+        double mv[COMBINE_G_BATCH][P];
+#pragma unroll
+        for (int t = 0; t < COMBINE_G_BATCH; ++t) {
+          const long long mo = (long long)sr[ef + min(q0 + t, ne - 1)] * a.m_stride;
+#pragma unroll
+          for (int p = 0; p < P; ++p) mv[t][p] = __ldcg(a.M + mo + mofs[p]);
+        }
+#pragma unroll
+        for (int t = 0; t < COMBINE_G_BATCH; ++t) {
+          if (q0 + t >= ne) break;
+          const int mk = sm[ef + q0 + t];
+          int k = mk >> 8;
+#pragma unroll
+          for (int q = 0; q < COMBINE_GROUP; ++q)
+            if (mk & (1 << q)) {
+              const double w = sc[k++];
+#pragma unroll
+              for (int p = 0; p < P; ++p) c[q][p] = fma(w, mv[t][p], c[q][p]);
+            }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < COMBINE_GROUP; ++q)
+        if (q < nm) {
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            if (live[p]) a.C[cb[q] + cofs[p]] = c[q][p];
+        }
+    }
+  }
+}
 
 // M_Add: C_l += sum_r W[l, r] * M_r for every C block l, products applied in order r.
 struct ScatterArgs {

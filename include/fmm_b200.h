@@ -131,10 +131,14 @@ long long fmm_last_workspace_bytes(void);
  *     FMM_E_TIMEOUT after the limit, stops waiting for tickets, and finishes (its result
  *     is then unreliable); fmm_device_status() reports it.  Lets a test check the
  *     timeout path without a fault.
- * Process-wide settings for tests; restore both before other work.  FMM_E_INVALID for an
- * unknown setting or a fill outside 0..255. */
+ *   FMM_DEBUG_COMBINE_POSITIONS: element positions each thread of the stored-products
+ *     combine pass owns (1 or 2; 0 restores the default of 1); results are unchanged, for
+ *     launch-shape sweeps.
+ * Process-wide settings for tests; restore them before other work.  FMM_E_INVALID for an
+ * unknown setting, a fill outside 0..255 or a position count outside 0..2. */
 #define FMM_DEBUG_WAIT_LIMIT_NS 1
 #define FMM_DEBUG_TICKET_FILL 2
+#define FMM_DEBUG_COMBINE_POSITIONS 3
 int fmm_debug_set(int what, long long value);
 
 /* FMM C += A*B (pack type ABC) that allocates no memory -- no counterpart in the
