@@ -872,10 +872,13 @@ std::atomic<int> g_combine_positions{0};
 int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long long ldc, int ms, int ns,
                    const double* M, long long ldm, long long m_stride, cudaStream_t st) {
   int dev = 0;
-  FMM_CUDA_TRY(cudaGetDevice(&dev));
+  int rc0 = configure_kernel(&dev);
+  if (rc0 != FMM_OK) return rc0;
   {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (!combine_configured[dev]) {
+      FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024));
       FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         200 * 1024));
       FMM_CUDA_TRY(cudaFuncSetAttribute(fmm::fmm_combine_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -899,6 +902,21 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
   ga.er = d.cg_r;
   ga.em = d.cg_m;
   ga.ec = d.cg_c;
+  const long long total = (long long)ms * ns;
+  const size_t ssm = fmm::combine_staged_smem_bytes(ga.ngroup, ga.nent, ga.ncoef);
+  // staged form: the M tiles of a position range are contiguous 16-byte-aligned runs
+  const bool staged = g_combine_positions.load() == 0 && ldm == ms && m_stride % 2 == 0 && total % 2 == 0 &&
+                      ((uintptr_t)M & 15) == 0 && ssm <= 200 * 1024 && total > 0;
+  if (staged) {
+    const long long ntile = (total + fmm::CST_TILE - 1) / fmm::CST_TILE;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(ntile, (long long)sm_count[dev] * 2));
+    {
+      ProfScope pf(K_COMBINE, st);
+      fmm::fmm_combine_staged_kernel<<<grid, fmm::CST_THREADS + 32, ssm, st>>>(ga, dev_status[dev]);
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return cuda_status(cudaGetLastError());
+  }
   const int P = g_combine_positions.load() == 2 ? 2 : 1;
   const size_t smem = fmm::combine_group_smem_bytes(ga.ngroup, ga.nent, ga.ncoef);
   const long long per = (long long)fmm::COMBINE_G_THREADS * P;

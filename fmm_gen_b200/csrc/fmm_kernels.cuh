@@ -1725,6 +1725,129 @@ __global__ void __launch_bounds__(COMBINE_G_THREADS) fmm_combine_kernel(const Co
   }
 }
 
+// The same combine with the M values staged in shared memory by bulk copies: a tile of
+// CST_TILE consecutive element positions (M_r[e0 .. e0 + CST_TILE) is contiguous when
+// ldm == ms), walked group by group and, within a group, CST_CHUNK products at a time; a
+// producer warp copies each chunk's M_r tiles (cp.async.bulk, 2 KB each) into a ring of
+// CST_STAGES stages while the compute warps apply earlier chunks, so the loads in flight per
+// SM are bounded by shared memory instead of registers.  A compute thread owns one position
+// of the tile and keeps its group's running C values in registers; the arithmetic per block
+// is the register kernel's (bit-identical).  Waits are bounded (status word on timeout).
+constexpr int CST_THREADS = 256;  // compute threads, one position each
+constexpr int CST_TILE = CST_THREADS;
+constexpr int CST_CHUNK = 8;      // products per stage
+constexpr int CST_STAGES = 6;
+constexpr size_t CST_STAGE_DOUBLES = (size_t)CST_CHUNK * CST_TILE;
+
+__host__ __device__ constexpr size_t combine_staged_smem_bytes(int ngroup, int nent, int ncoef) {
+  return sizeof(double) * CST_STAGE_DOUBLES * CST_STAGES + 16 * CST_STAGES +
+         combine_group_smem_bytes(ngroup, nent, ncoef);
+}
+
+__device__ __forceinline__ void bulk_load_1d(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// CombineGroupArgs plus the status word; requires ldm == ms, M and m_stride 16-byte
+// multiples (in doubles: m_stride even) and ms * ns even (every tile's byte count a multiple
+// of 16).
+__global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(const CombineGroupArgs a,
+                                                                              unsigned* status) {
+  extern __shared__ __align__(128) double cst[];
+  double* stages = cst;                                                    // [STAGES][CHUNK][TILE]
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(stages + CST_STAGE_DOUBLES * CST_STAGES);
+  double* sc = reinterpret_cast<double*>(bars + 2 * CST_STAGES);           // [ncoef]
+  int* sr = reinterpret_cast<int*>(sc + a.ncoef);                          // [nent]
+  int* sm = sr + a.nent;                                                   // [nent]
+  int* sg = sm + a.nent;                                                   // [GDESC * ngroup]
+  const unsigned full0 = smem_u32(bars), empty0 = smem_u32(bars + CST_STAGES);
+  const int tid = threadIdx.x;
+  for (int q = tid; q < a.ncoef; q += blockDim.x) sc[q] = a.ec[q];
+  for (int q = tid; q < a.nent; q += blockDim.x) {
+    sr[q] = a.er[q];
+    sm[q] = a.em[q];
+  }
+  for (int q = tid; q < GDESC * a.ngroup; q += blockDim.x) sg[q] = a.gdesc[q];
+  if (tid == 0) {
+    for (int s = 0; s < CST_STAGES; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, CST_THREADS / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const long long total = (long long)a.ms * a.ns;
+  const long long ntile = (total + CST_TILE - 1) / CST_TILE;
+  long long k = 0;  // stage step of this CTA
+  if (tid >= CST_THREADS) {  // producer warp: lane 0 issues the copies
+    if (tid != CST_THREADS) return;
+    for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
+      const long long e0 = t * CST_TILE;
+      const unsigned bytes = (unsigned)(8 * min((long long)CST_TILE, total - e0));
+      for (int g = 0; g < a.ngroup; ++g) {
+        const int ef = sg[g * GDESC], ne = sg[g * GDESC + 1];
+        for (int q0 = 0; q0 < ne; q0 += CST_CHUNK, ++k) {
+          const int s = (int)(k % CST_STAGES);
+          mbar_wait(empty0 + 8 * s, (unsigned)(((k / CST_STAGES) & 1) ^ 1), status);
+          const int nq = min(CST_CHUNK, ne - q0);
+          mbar_arrive_expect_tx(full0 + 8 * s, bytes * nq);
+          for (int q = 0; q < nq; ++q)
+            bulk_load_1d(smem_u32(stages + (size_t)s * CST_STAGE_DOUBLES + (size_t)q * CST_TILE),
+                         a.M + (long long)sr[ef + q0 + q] * a.m_stride + e0, bytes, full0 + 8 * s);
+        }
+      }
+    }
+    // copies still in flight (only on an error path) land before the CTA exits
+    for (long long q = k - CST_STAGES; q < k; ++q)
+      if (q >= 0) mbar_wait_drain(full0 + 8 * (int)(q % CST_STAGES), (unsigned)((q / CST_STAGES) & 1));
+    return;
+  }
+  const int lane = tid & 31;
+  for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const long long e = t * CST_TILE + tid;
+    const bool live = e < total;
+    const long long ee = live ? e : total - 1;
+    const long long cofs = (ee % a.ms) + (ee / a.ms) * a.ldc;
+    for (int g = 0; g < a.ngroup; ++g) {
+      const int* gd = sg + g * GDESC;
+      const int ef = gd[0], ne = gd[1], nm = gd[2];
+      double c[COMBINE_GROUP];
+      long long cb[COMBINE_GROUP];
+#pragma unroll
+      for (int q = 0; q < COMBINE_GROUP; ++q) {
+        const int b = gd[4 + (q < nm ? q : 0)];
+        cb[q] = (long long)(b / a.grid_n) * a.ms + (long long)(b % a.grid_n) * a.ns * a.ldc + cofs;
+        c[q] = q < nm ? a.C[cb[q]] : 0.0;
+      }
+      for (int q0 = 0; q0 < ne; q0 += CST_CHUNK, ++k) {
+        const int s = (int)(k % CST_STAGES);
+        mbar_wait(full0 + 8 * s, (unsigned)((k / CST_STAGES) & 1), status);
+        const double* st = stages + (size_t)s * CST_STAGE_DOUBLES + tid;
+        const int nq = min(CST_CHUNK, ne - q0);
+#pragma unroll
+        for (int q = 0; q < CST_CHUNK; ++q) {
+          if (q >= nq) break;
+          const double m = st[(size_t)q * CST_TILE];
+          const int mk = sm[ef + q0 + q];
+          int kc = mk >> 8;
+#pragma unroll
+          for (int b = 0; b < COMBINE_GROUP; ++b)
+            if (mk & (1 << b)) c[b] = fma(sc[kc++], m, c[b]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * s);
+      }
+      if (live) {
+#pragma unroll
+        for (int q = 0; q < COMBINE_GROUP; ++q)
+          if (q < nm) a.C[cb[q]] = c[q];
+      }
+    }
+  }
+}
+
 // M_Add: C_l += sum_r W[l, r] * M_r for every C block l, products applied in order r.
 struct ScatterArgs {
   double* C;

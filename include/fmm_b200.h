@@ -131,9 +131,9 @@ long long fmm_last_workspace_bytes(void);
  *     FMM_E_TIMEOUT after the limit, stops waiting for tickets, and finishes (its result
  *     is then unreliable); fmm_device_status() reports it.  Lets a test check the
  *     timeout path without a fault.
- *   FMM_DEBUG_COMBINE_POSITIONS: element positions each thread of the stored-products
- *     combine pass owns (1 or 2; 0 restores the default of 1); results are unchanged, for
- *     launch-shape sweeps.
+ *   FMM_DEBUG_COMBINE_POSITIONS: form of the stored-products combine pass: 0 (default) the
+ *     shared-memory-staged form where the operands allow it, 1 or 2 the register form with
+ *     that many element positions per thread; results are unchanged, for sweeps.
  * Process-wide settings for tests; restore them before other work.  FMM_E_INVALID for an
  * unknown setting, a fill outside 0..255 or a position count outside 0..2. */
 #define FMM_DEBUG_WAIT_LIMIT_NS 1
