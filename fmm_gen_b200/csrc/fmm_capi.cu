@@ -107,6 +107,9 @@ struct DevTables {
   int* cg_r = nullptr;
   int* cg_m = nullptr;
   double* cg_c = nullptr;
+  int* ch_r = nullptr;
+  unsigned long long* ch_m = nullptr;
+  double* ch_c = nullptr;
   fmm::Prod* prods_ps = nullptr;  // products over pre-summed operands (one A and one B term each)
   fmm::Term* terms_ps = nullptr;
   int* plistA = nullptr;          // products whose A operand is pre-summed, in slot order
@@ -144,6 +147,9 @@ struct fmm_plan {
   std::vector<int> cg_desc, cg_r, cg_m;
   std::vector<double> cg_c;
   int n_cgroup = 0;
+  std::vector<int> ch_r;                 // staged kernel: CST_CHUNK products per chunk
+  std::vector<unsigned long long> ch_m;  // one byte of slot bits per member
+  std::vector<double> ch_c;              // COMBINE_GROUP x CST_CHUNK coefficients per chunk
   // Pre-summed form: each product's A operand is either its single A block (src 0) or
   // slot j of the workspace S (src 1) that holds sum_i U[i,r] A_i; likewise for B / T.
   std::vector<fmm::Prod> prods_ps;
@@ -202,6 +208,9 @@ int upload_tables(fmm_plan* p, DevTables& d) {
     FMM_CUDA_TRY(up(&d.cg_r, p->cg_r));
     FMM_CUDA_TRY(up(&d.cg_m, p->cg_m));
     FMM_CUDA_TRY(up(&d.cg_c, p->cg_c));
+    FMM_CUDA_TRY(up(&d.ch_r, p->ch_r));
+    FMM_CUDA_TRY(up(&d.ch_m, p->ch_m));
+    FMM_CUDA_TRY(up(&d.ch_c, p->ch_c));
   }
   FMM_CUDA_TRY(cudaMalloc(&d.prods_ps, sizeof(fmm::Prod) * p->prods_ps.size()));
   FMM_CUDA_TRY(cudaMalloc(&d.terms_ps, sizeof(fmm::Term) * p->terms_ps.size()));
@@ -405,11 +414,14 @@ void build_combine_groups(fmm_plan* p) {
     uni = u2;
   }
   p->cg_desc.clear();
+  p->ch_r.clear();
+  p->ch_m.clear();
+  p->ch_c.clear();
   p->cg_r.clear();
   p->cg_m.clear();
   p->cg_c.clear();
   for (size_t g = 0; g < mem.size(); ++g) {
-    const int first = (int)p->cg_r.size(), firstc = (int)p->cg_c.size();
+    const int first = (int)p->cg_r.size();
     std::vector<size_t> pos(mem[g].size(), 0);  // cursor into each member's (increasing r) list
     for (int r : uni[g]) {
       int mask = 0;
@@ -426,16 +438,55 @@ void build_combine_groups(fmm_plan* p) {
       p->cg_r.push_back(r);
       p->cg_m.push_back(mask | (k0 << 8));
     }
+    // the group's entries in chunks of CST_CHUNK (the staged kernel's stage): per chunk the
+    // products, one byte per member (bit t: slot t updates it) and a member-major
+    // CST_CHUNK x CST_CHUNK coefficient block (0 where the bit is clear)
+    const int first_chunk = (int)(p->ch_r.size() / fmm::CST_CHUNK);
+    {
+      const int ne = (int)p->cg_r.size() - first;
+      for (int q0 = 0; q0 < ne; q0 += fmm::CST_CHUNK) {
+        unsigned long long bits = 0;
+        std::vector<double> cf((size_t)fmm::COMBINE_GROUP * fmm::CST_CHUNK, 0.0);
+        for (int t = 0; t < fmm::CST_CHUNK; ++t) {
+          const int e = first + std::min(q0 + t, ne - 1);
+          p->ch_r.push_back(p->cg_r[e]);
+          if (q0 + t >= ne) continue;
+          const int mk = p->cg_m[e];
+          int kc = mk >> 8;
+          for (int q = 0; q < fmm::COMBINE_GROUP; ++q)
+            if (mk & (1 << q)) {
+              bits |= 1ULL << (8 * q + t);
+              cf[(size_t)q * fmm::CST_CHUNK + t] = p->cg_c[kc++];
+            }
+        }
+        p->ch_m.push_back(bits);
+        p->ch_c.insert(p->ch_c.end(), cf.begin(), cf.end());
+      }
+    }
     p->cg_desc.push_back(first);
     p->cg_desc.push_back((int)p->cg_r.size() - first);
     p->cg_desc.push_back((int)mem[g].size());
-    p->cg_desc.push_back(firstc);
+    p->cg_desc.push_back(first_chunk);
     for (int q = 0; q < fmm::COMBINE_GROUP; ++q) {
       const int b = q < (int)mem[g].size() ? mem[g][q] : mem[g][0];
       p->cg_desc.push_back(p->cblk[4 * b] * p->dims[2] + p->cblk[4 * b + 1]);
     }
   }
   p->n_cgroup = (int)mem.size();
+  // the kernels index their tables with these values: check them here (a plan whose tables
+  // fail falls back to the per-block scatter)
+  bool ok = p->ch_r.size() == (size_t)fmm::CST_CHUNK * p->ch_m.size() &&
+            p->ch_c.size() == (size_t)fmm::COMBINE_GROUP * fmm::CST_CHUNK * p->ch_m.size();
+  for (int r : p->ch_r) ok = ok && r >= 0 && r < p->rank;
+  for (int r : p->cg_r) ok = ok && r >= 0 && r < p->rank;
+  for (int g = 0; ok && g < p->n_cgroup; ++g) {
+    const int* gd = p->cg_desc.data() + (size_t)g * fmm::GDESC;
+    const int nch = (gd[1] + fmm::CST_CHUNK - 1) / fmm::CST_CHUNK;
+    ok = gd[1] > 0 && gd[0] + gd[1] <= (int)p->cg_r.size() && gd[2] >= 1 && gd[2] <= fmm::COMBINE_GROUP &&
+         gd[3] >= 0 && gd[3] + nch <= (int)p->ch_m.size();
+    for (int q = 0; ok && q < fmm::COMBINE_GROUP; ++q) ok = gd[4 + q] >= 0 && gd[4 + q] < p->dims[0] * p->dims[2];
+  }
+  if (!ok) p->n_cgroup = 0;
 }
 
 int build_plan(const int dims[3], int rank, const int* nterms, const int* rows, const int* cols,
@@ -902,8 +953,13 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
   ga.er = d.cg_r;
   ga.em = d.cg_m;
   ga.ec = d.cg_c;
+  ga.nprod = plan->rank;
   const long long total = (long long)ms * ns;
-  const size_t ssm = fmm::combine_staged_smem_bytes(ga.ngroup, ga.nent, ga.ncoef);
+  ga.nchunk = (int)plan->ch_m.size();
+  ga.chr = d.ch_r;
+  ga.chm = d.ch_m;
+  ga.chc = d.ch_c;
+  const size_t ssm = fmm::combine_staged_smem_bytes(ga.ngroup, ga.nchunk);
   // staged form: the M tiles of a position range are contiguous 16-byte-aligned runs
   const bool staged = g_combine_positions.load() == 0 && ldm == ms && m_stride % 2 == 0 && total % 2 == 0 &&
                       ((uintptr_t)M & 15) == 0 && ssm <= 200 * 1024 && total > 0;
@@ -949,19 +1005,25 @@ bool use_presum(const fmm_plan* plan, int ms, int ns, int ks) {
 // to a workspace and one combine pass (every M_r and C element crossing HBM once).  The
 // epilogue moves 16 nnz(W) ms ns bytes of C while the DMMAs run; the stored schedule writes
 // 8 R ms ns bytes of product tiles (also during the DMMAs), then the combine pass moves
-// 8 (R + 2 blocks) ms ns bytes.  Rates measured on B200: DMMA products 33 TFLOP/s executed,
-// the epilogue's C traffic 4.6 TB/s (222-1 x 333-1 at 14400 x 14400 x 480: 55.7 GB in
-// 12.2 ms), product stores 6 TB/s, the combine pass 3.3 TB/s.  The stored schedule must
-// gain 10 %.  It is the reference's own trade between its ABC and AB variants
-// (meta/model_gen.py:87-95 counts the C memory operations of each).
+// 8 (R + 2 blocks) ms ns bytes.  Model fitted to B200 measurements (222-1 x 333-1, DMMA
+// products 33 TFLOP/s executed, epilogue C traffic 4.6 TB/s, product stores 6 TB/s, combine
+// 2.6 TB/s): the direct launch takes max(t_mma, t_epi) + 1.05 min^2 / max (the two overlap
+// less as they approach each other: 4000 x 16000 x 2000 7.76 ms for t_mma 5.75 and t_epi
+// 3.32, 14400 x 14400 x 480 12.4 ms, 8192^3 24.2 ms), the storing launch 1.08 max(t_mma,
+// t_store) (6.16 and 4.92 ms).  The stored schedule must gain 3 % and its product workspace
+// (8 R ms ns bytes) must fit the workspace cap.  It is the reference's own trade between its
+// ABC and AB variants (meta/model_gen.py:87-95 counts the C memory operations of each).
 bool prefer_stored_products(const fmm_plan* plan, int ms, int ns, int ks) {
   const double mn = (double)ms * ns;
   const int nblk = plan->dims[0] * plan->dims[2];
+  if (8.0 * plan->rank * mn > (double)g_ws_limit.load()) return false;
   const double t_mma = 2.0 * plan->rank * mn * ks / 33e12;
   const double t_epi = 16.0 * plan->n_cterms * mn / 4.6e12;
   const double t_store = 8.0 * plan->rank * mn / 6.0e12;
-  const double t_comb = 8.0 * (plan->rank + 2.0 * nblk) * mn / 3.3e12;
-  return std::max(t_mma, t_store) + t_comb < 0.9 * std::max(t_mma, t_epi);
+  const double t_comb = 8.0 * (plan->rank + 2.0 * nblk) * mn / 2.6e12;
+  const double hi = std::max(t_mma, t_epi), lo = std::min(t_mma, t_epi);
+  const double t_direct = hi + 1.05 * lo * lo / hi;
+  return 1.08 * std::max(t_mma, t_store) + t_comb < 0.97 * t_direct;
 }
 
 int presum(const DevTables& d, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
@@ -1360,6 +1422,7 @@ int device_status(bool clear) {
   }
   const int rn = noalloc_status(dev, clear);
   if (rn != FMM_OK && rn != FMM_E_TIMEOUT) return rn;
+  if (v & fmm::STATUS_TABLE) return FMM_E_PLAN;
   return (v || rn == FMM_E_TIMEOUT) ? FMM_E_TIMEOUT : FMM_OK;
 }
 
@@ -1537,6 +1600,9 @@ int fmm_plan_destroy(fmm_plan* plan) {
     cudaFree(d.cg_r);
     cudaFree(d.cg_m);
     cudaFree(d.cg_c);
+    cudaFree(d.ch_r);
+    cudaFree(d.ch_m);
+    cudaFree(d.ch_c);
     cudaFree(d.prods_ps);
     cudaFree(d.terms_ps);
     cudaFree(d.plistA);
@@ -1554,6 +1620,14 @@ int fmm_plan_destroy(fmm_plan* plan) {
 }
 
 int fmm_plan_rank(const fmm_plan* plan) { return plan ? plan->rank : FMM_E_INVALID; }
+
+int fmm_plan_combine_info(const fmm_plan* plan, int* groups, int* entries, int* chunks) {
+  if (!plan) return FMM_E_INVALID;
+  if (groups) *groups = plan->n_cgroup;
+  if (entries) *entries = plan->n_cgroup ? (int)plan->cg_r.size() : 0;
+  if (chunks) *chunks = plan->n_cgroup ? (int)plan->ch_m.size() : 0;
+  return FMM_OK;
+}
 
 int fmm_bind_default_plan(fmm_plan* plan) {
   std::lock_guard<std::mutex> lk(g_default_mu);

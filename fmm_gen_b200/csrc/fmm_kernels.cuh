@@ -120,7 +120,8 @@ enum Mode : int { MODE_ACCUM_C = 0, MODE_STORE_M = 1 };
 // STATUS_TICKET_TIMEOUT: a wait for another CTA's C updates gave up (the kernel finishes,
 // without the product order from then on); STATUS_WAIT_TIMEOUT: a wait inside a CTA's own
 // pipeline gave up (every later wait returns at once and the kernel winds down).
-enum StatusBits : unsigned { STATUS_TICKET_TIMEOUT = 1u, STATUS_WAIT_TIMEOUT = 2u };
+// STATUS_TABLE: a kernel found an index outside its tables (clamped; the result is void)
+enum StatusBits : unsigned { STATUS_TICKET_TIMEOUT = 1u, STATUS_WAIT_TIMEOUT = 2u, STATUS_TABLE = 4u };
 
 // Time limit of the bounded device-side waits in ns: WAIT_LIMIT_NS unless a test lowers it
 // (fmm_debug_set); read only on a wait's slow path.
@@ -1618,7 +1619,7 @@ __global__ void fmm_pitch_copy1_kernel(const PitchCopy t) { pitch_copy_body(t); 
 // direct schedule.  The host groups blocks that share products (greedy by overlap), which
 // cuts the M loads per position from nnz(W) toward R (222-1 x 333-1: 540 -> 299 in 5
 // groups) with no shared-memory read-modify-write.  Tables (shared memory, per CTA):
-//   group g: gdesc[g * GDESC + 0..3] = first entry, #entries, #members, first coefficient;
+//   group g: gdesc[g * GDESC + 0..3] = first entry, #entries, #members, first chunk;
 //            gdesc[g * GDESC + 4 + q] = block id of member q (row * grid_n + col)
 //   entry e: er[e] = product r, em[e] = member mask | (first coefficient of e) << 8,
 //            the coefficients of its set bits, member order, from ec[first coefficient]
@@ -1640,6 +1641,12 @@ struct CombineGroupArgs {
   const int* er;
   const int* em;
   const double* ec;
+  int nprod;  // products (slabs of M)
+  // staged kernel: the entries of each group in chunks of CST_CHUNK
+  int nchunk;
+  const int* chr;                 // [nchunk][CST_CHUNK] products (past a group's end: its last)
+  const unsigned long long* chm;  // [nchunk] byte q: slots that update member q
+  const double* chc;              // [nchunk][COMBINE_GROUP][CST_CHUNK] coefficients
 };
 
 __host__ __device__ constexpr size_t combine_group_smem_bytes(int ngroup, int nent, int ncoef) {
@@ -1736,12 +1743,15 @@ __global__ void __launch_bounds__(COMBINE_G_THREADS) fmm_combine_kernel(const Co
 constexpr int CST_THREADS = 256;  // compute threads, one position each
 constexpr int CST_TILE = CST_THREADS;
 constexpr int CST_CHUNK = 8;      // products per stage
-constexpr int CST_STAGES = 6;
+constexpr int CST_STAGES = 5;
 constexpr size_t CST_STAGE_DOUBLES = (size_t)CST_CHUNK * CST_TILE;
+static_assert(COMBINE_GROUP * CST_CHUNK <= 64, "one 64-bit word of slot bits per chunk");
 
-__host__ __device__ constexpr size_t combine_staged_smem_bytes(int ngroup, int nent, int ncoef) {
+__host__ __device__ constexpr size_t combine_staged_smem_bytes(int ngroup, int nchunk) {
   return sizeof(double) * CST_STAGE_DOUBLES * CST_STAGES + 16 * CST_STAGES +
-         combine_group_smem_bytes(ngroup, nent, ncoef);
+         (sizeof(double) * COMBINE_GROUP * CST_CHUNK + sizeof(unsigned long long) + sizeof(int) * CST_CHUNK) *
+             (size_t)nchunk +
+         sizeof(int) * GDESC * (size_t)ngroup + 16;
 }
 
 __device__ __forceinline__ void bulk_load_1d(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
@@ -1758,17 +1768,15 @@ __global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(co
   extern __shared__ __align__(128) double cst[];
   double* stages = cst;                                                    // [STAGES][CHUNK][TILE]
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(stages + CST_STAGE_DOUBLES * CST_STAGES);
-  double* sc = reinterpret_cast<double*>(bars + 2 * CST_STAGES);           // [ncoef]
-  int* sr = reinterpret_cast<int*>(sc + a.ncoef);                          // [nent]
-  int* sm = sr + a.nent;                                                   // [nent]
-  int* sg = sm + a.nent;                                                   // [GDESC * ngroup]
+  double* sc = reinterpret_cast<double*>(bars + 2 * CST_STAGES);           // [nchunk][GROUP][CHUNK]
+  unsigned long long* smk = reinterpret_cast<unsigned long long*>(sc + (size_t)a.nchunk * COMBINE_GROUP * CST_CHUNK);
+  int* sr = reinterpret_cast<int*>(smk + a.nchunk);                        // [nchunk][CHUNK]
+  int* sg = sr + (size_t)a.nchunk * CST_CHUNK;                             // [GDESC * ngroup]
   const unsigned full0 = smem_u32(bars), empty0 = smem_u32(bars + CST_STAGES);
   const int tid = threadIdx.x;
-  for (int q = tid; q < a.ncoef; q += blockDim.x) sc[q] = a.ec[q];
-  for (int q = tid; q < a.nent; q += blockDim.x) {
-    sr[q] = a.er[q];
-    sm[q] = a.em[q];
-  }
+  for (int q = tid; q < a.nchunk * COMBINE_GROUP * CST_CHUNK; q += blockDim.x) sc[q] = a.chc[q];
+  for (int q = tid; q < a.nchunk; q += blockDim.x) smk[q] = a.chm[q];
+  for (int q = tid; q < a.nchunk * CST_CHUNK; q += blockDim.x) sr[q] = a.chr[q];
   for (int q = tid; q < GDESC * a.ngroup; q += blockDim.x) sg[q] = a.gdesc[q];
   if (tid == 0) {
     for (int s = 0; s < CST_STAGES; ++s) {
@@ -1787,15 +1795,22 @@ __global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(co
       const long long e0 = t * CST_TILE;
       const unsigned bytes = (unsigned)(8 * min((long long)CST_TILE, total - e0));
       for (int g = 0; g < a.ngroup; ++g) {
-        const int ef = sg[g * GDESC], ne = sg[g * GDESC + 1];
+        const int ne = sg[g * GDESC + 1], c0 = sg[g * GDESC + 3];
         for (int q0 = 0; q0 < ne; q0 += CST_CHUNK, ++k) {
           const int s = (int)(k % CST_STAGES);
           mbar_wait(empty0 + 8 * s, (unsigned)(((k / CST_STAGES) & 1) ^ 1), status);
           const int nq = min(CST_CHUNK, ne - q0);
+          const int* rr = sr + (size_t)(c0 + q0 / CST_CHUNK) * CST_CHUNK;
           mbar_arrive_expect_tx(full0 + 8 * s, bytes * nq);
-          for (int q = 0; q < nq; ++q)
+          for (int q = 0; q < nq; ++q) {
+            int r = rr[q];
+            if ((unsigned)r >= (unsigned)a.nprod) {  // never with host-checked tables
+              atomicOr(status, STATUS_TABLE);
+              r = 0;
+            }
             bulk_load_1d(smem_u32(stages + (size_t)s * CST_STAGE_DOUBLES + (size_t)q * CST_TILE),
-                         a.M + (long long)sr[ef + q0 + q] * a.m_stride + e0, bytes, full0 + 8 * s);
+                         a.M + (long long)r * a.m_stride + e0, bytes, full0 + 8 * s);
+          }
         }
       }
     }
@@ -1812,7 +1827,7 @@ __global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(co
     const long long cofs = (ee % a.ms) + (ee / a.ms) * a.ldc;
     for (int g = 0; g < a.ngroup; ++g) {
       const int* gd = sg + g * GDESC;
-      const int ef = gd[0], ne = gd[1], nm = gd[2];
+      const int ne = gd[1], nm = gd[2], c0 = gd[3];
       double c[COMBINE_GROUP];
       long long cb[COMBINE_GROUP];
 #pragma unroll
@@ -1823,21 +1838,25 @@ __global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(co
       }
       for (int q0 = 0; q0 < ne; q0 += CST_CHUNK, ++k) {
         const int s = (int)(k % CST_STAGES);
+        const int ch = c0 + q0 / CST_CHUNK;
+        const unsigned long long bits = smk[ch];
+        const double* cf = sc + (size_t)ch * COMBINE_GROUP * CST_CHUNK;
         mbar_wait(full0 + 8 * s, (unsigned)((k / CST_STAGES) & 1), status);
         const double* st = stages + (size_t)s * CST_STAGE_DOUBLES + tid;
-        const int nq = min(CST_CHUNK, ne - q0);
+        double m[CST_CHUNK];  // slots past the group's end hold stale data and have no bits
 #pragma unroll
-        for (int q = 0; q < CST_CHUNK; ++q) {
-          if (q >= nq) break;
-          const double m = st[(size_t)q * CST_TILE];
-          const int mk = sm[ef + q0 + q];
-          int kc = mk >> 8;
-#pragma unroll
-          for (int b = 0; b < COMBINE_GROUP; ++b)
-            if (mk & (1 << b)) c[b] = fma(sc[kc++], m, c[b]);
-        }
+        for (int q = 0; q < CST_CHUNK; ++q) m[q] = st[(size_t)q * CST_TILE];
+        __threadfence_block();  // the stage's loads complete before it can be refilled
         __syncwarp();
-        if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        if (lane == 0) mbar_arrive(empty0 + 8 * s);  // the stage's values are in registers
+#pragma unroll
+        for (int b = 0; b < COMBINE_GROUP; ++b) {
+          const unsigned bq = (unsigned)(bits >> (8 * b)) & 0xffu;
+          if (bq == 0) continue;
+#pragma unroll
+          for (int q = 0; q < CST_CHUNK; ++q)
+            if (bq & (1u << q)) c[b] = fma(cf[b * CST_CHUNK + q], m[q], c[b]);
+        }
       }
       if (live) {
 #pragma unroll

@@ -71,6 +71,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.fmm_plan_destroy.restype = c_int
     lib.fmm_plan_rank.argtypes = [c_void_p]
     lib.fmm_plan_rank.restype = c_int
+    lib.fmm_plan_combine_info.argtypes = [c_void_p, c_int_p, c_int_p, c_int_p]
+    lib.fmm_plan_combine_info.restype = c_int
     lib.fmm_bind_default_plan.argtypes = [c_void_p]
     lib.fmm_bind_default_plan.restype = c_int
     lib.fmm_default_plan.argtypes = []

@@ -78,6 +78,11 @@ int fmm_plan_create(const int dims[3], int rank, const int *nterms, const int *r
                     const double *coefs, fmm_plan **out);
 int fmm_plan_destroy(fmm_plan *plan);
 int fmm_plan_rank(const fmm_plan *plan);
+/* The stored-products combine pass's tables of a plan (no counterpart in the reference):
+ * C blocks in groups that share products, the merged entries (one per product of a
+ * group's union) and their chunks of 8.  groups = 0: the tables did not pass their checks
+ * and the per-block scatter runs instead.  Any output pointer may be NULL. */
+int fmm_plan_combine_info(const fmm_plan *plan, int *groups, int *entries, int *chunks);
 int fmm_bind_default_plan(fmm_plan *plan);
 fmm_plan *fmm_default_plan(void);
 

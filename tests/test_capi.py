@@ -87,3 +87,19 @@ def test_python_layer_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(runtime, "_lib", None)
     with pytest.raises(runtime.FmmError):
         runtime.load_library()
+
+
+@pytest.mark.parametrize("algs,levels,groups,entries", [
+    (["222", "333"], [1, 1], 5, 299),  # greedy grouping of the 36 C blocks (nnz(W) = 540)
+    (["222"], [2], 2, 81),              # 16 blocks, nnz(W) = 144
+    (["222"], [1], 1, 7),
+])
+def test_combine_tables_group_blocks_that_share_products(lib, algs, levels, groups, entries):
+    """The combine pass's grouped tables pass their own checks (else the scatter would run)
+    and merge each group's products: fewer M loads per position than nnz(W)."""
+    p = runtime.Plan(algebra.make_plan(algs, levels))
+    g, e, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert lib.fmm_plan_combine_info(p.handle, ctypes.byref(g), ctypes.byref(e), ctypes.byref(c)) == 0
+    assert (g.value, e.value) == (groups, entries)
+    assert c.value >= (entries + 7) // 8 and c.value <= entries // 8 + groups
+    p.close()
