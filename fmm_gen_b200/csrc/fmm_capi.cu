@@ -1428,32 +1428,44 @@ int device_status(bool clear) {
 
 // Host-pointer execution: stage A, B, C into device memory, run, copy C back.
 //
-// Large problems run as column panels C[:, J] += A * B[:, J], each a GEMM of its own
-// (partitioned like any m x |J| x k call), so that the copies overlap the compute: A goes
-// in first, then panel j computes on the calling thread's stream while panel j+1's B and
-// C come in on one copy stream and panel j-1's C goes back on another (host-to-device and
-// device-to-host copies run at the same time).  With P panels only A plus one panel's B
-// and C are copied before the first kernel, and one panel's C after the last.  Panel
-// edges fall on multiples of 128 x (block columns of the plan), so every panel's
-// sub-blocks are whole 128-column tiles where the width allows.
+// Large problems run as a grid of R row panels x P column panels of C, each block
+// C[I, J] += A[I, :] * B[:, J] a GEMM of its own (partitioned like any |I| x |J| x k call), so
+// that the copies overlap the compute.  Blocks run column panel by column panel, the row
+// panels inside: the copy-in stream brings, in that order, each block's operands that are not
+// on the device yet (A[I, :] at its first use, B[:, J] at its first use, C[I, J]); the
+// calling thread's stream computes block b once its copies have landed while the next
+// blocks' operands come in; a copy-out stream returns C[I, J] after its block (host-to-
+// device and device-to-host copies run at the same time).  Before the first kernel only
+// A[I_0, :], B[:, J_0] and C[I_0, J_0] are copied: with two row panels half of A instead of
+// all of it (16384^3: 1.8 instead of 3.2 GB).  Row and column edges fall on multiples of 128 x
+// (block rows / columns of the plan), so every block's sub-blocks are whole 128-row tiles
+// where the size allows.
 #ifndef FMM_HOST_PANELS
 #define FMM_HOST_PANELS 4
 #endif
-constexpr int kHostPanelMinCols = 2048;              // panels at least this wide
+constexpr int kHostPanelMinCols = 2048;              // column panels at least this wide
 constexpr long long kHostPanelMinElems = 1LL << 22;  // C of at least 32 MB
+constexpr long long kHostRowSplitMinA = 1LL << 26;   // two row panels once A has 2^26 elements (512 MB)
+constexpr int kHostRowPanelMinRows = 4096;
 
-int host_panels(const fmm_plan* plan, bool plain, int m, int n, std::vector<int>* edges) {
-  int P = 1;
-  if ((long long)m * n >= kHostPanelMinElems) P = std::max(1, std::min(FMM_HOST_PANELS, n / kHostPanelMinCols));
-  const int unit = 128 * ((plain || !plan) ? 1 : plan->dims[2]);
+void split_edges(int total, int parts, int unit, std::vector<int>* edges) {
   edges->assign(1, 0);
-  for (int j = 1; j < P; ++j) {
-    long long e = (long long)n * j / P;
-    if (n / P >= unit) e -= e % unit;
-    if (e > edges->back() && e < n) edges->push_back((int)e);
+  for (int j = 1; j < parts; ++j) {
+    long long e = (long long)total * j / parts;
+    if (total / parts >= unit) e -= e % unit;
+    if (e > edges->back() && e < total) edges->push_back((int)e);
   }
-  edges->push_back(n);
-  return (int)edges->size() - 1;
+  edges->push_back(total);
+}
+
+int host_panels(const fmm_plan* plan, bool plain, int m, int n, int k, std::vector<int>* rows,
+                std::vector<int>* cols) {
+  int P = 1, R = 1;
+  if ((long long)m * n >= kHostPanelMinElems) P = std::max(1, std::min(FMM_HOST_PANELS, n / kHostPanelMinCols));
+  if (P > 1 && (long long)m * k >= kHostRowSplitMinA && m >= 2 * kHostRowPanelMinRows) R = 2;
+  split_edges(m, R, 128 * ((plain || !plan) ? 1 : plan->dims[0]), rows);
+  split_edges(n, P, 128 * ((plain || !plan) ? 1 : plan->dims[2]), cols);
+  return (int)(rows->size() - 1) * (int)(cols->size() - 1);
 }
 
 int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, const double* A, int lda,
@@ -1467,47 +1479,54 @@ int run_host(const fmm_plan* plan, int pack, bool plain, int m, int n, int k, co
   const int pa = m + (m & 1), pb = k + (k & 1);
   const size_t szA = sizeof(double) * (size_t)pa * k, szB = sizeof(double) * (size_t)pb * n,
                szC = sizeof(double) * (size_t)m * n;
-  std::vector<int> edges;
-  const int P = host_panels(plan, plain, m, n, &edges);
+  std::vector<int> re, ce;
+  const int NB = host_panels(plan, plain, m, n, k, &re, &ce);
+  const int R = (int)re.size() - 1;
   double *dA = nullptr, *dB = nullptr, *dC = nullptr;
   cudaStream_t sin = nullptr, sout = nullptr;
-  std::vector<cudaEvent_t> ev;  // [0]: allocations made; [1 + j]: panel j copied in; [1 + P + j]: panel j done
+  std::vector<cudaEvent_t> ev;  // [0]: allocations made; [1 + b]: block b copied in; [1 + NB + b]: block b done
   auto ok = [&](cudaError_t e) {
     if (rc == FMM_OK && e != cudaSuccess) rc = cuda_status(e);
     return rc == FMM_OK;
   };
   ok(cudaMallocAsync((void**)&dA, szA, st)) && ok(cudaMallocAsync((void**)&dB, szB, st)) &&
       ok(cudaMallocAsync((void**)&dC, szC, st));
-  if (rc == FMM_OK && P > 1) {
+  if (rc == FMM_OK && NB > 1) {
     ok(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking)) &&
         ok(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking));
-    ev.assign(1 + 2 * P, nullptr);
+    ev.assign(1 + 2 * NB, nullptr);
     for (auto& e : ev)
       if (!ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) break;
   }
-  cudaStream_t cin = P > 1 ? sin : st, cout = P > 1 ? sout : st;
-  if (rc == FMM_OK && P > 1) ok(cudaEventRecord(ev[0], st)) && ok(cudaStreamWaitEvent(sin, ev[0], 0));
-  if (rc == FMM_OK)
-    ok(cudaMemcpy2DAsync(dA, sizeof(double) * pa, A, sizeof(double) * lda, sizeof(double) * m, k,
-                         cudaMemcpyHostToDevice, cin));
-  for (int j = 0; j < P && rc == FMM_OK; ++j) {
-    const int c0 = edges[j], nj = edges[j + 1] - edges[j];
-    ok(cudaMemcpy2DAsync(dB + (size_t)c0 * pb, sizeof(double) * pb, B + (size_t)c0 * ldb, sizeof(double) * ldb,
-                         sizeof(double) * k, nj, cudaMemcpyHostToDevice, cin)) &&
-        ok(cudaMemcpy2DAsync(dC + (size_t)c0 * m, sizeof(double) * m, C + (size_t)c0 * ldc, sizeof(double) * ldc,
-                             sizeof(double) * m, nj, cudaMemcpyHostToDevice, cin));
-    if (P > 1 && rc == FMM_OK) ok(cudaEventRecord(ev[1 + j], sin));
-  }
-  for (int j = 0; j < P && rc == FMM_OK; ++j) {
-    const int c0 = edges[j], nj = edges[j + 1] - edges[j];
-    if (P > 1 && !ok(cudaStreamWaitEvent(st, ev[1 + j], 0))) break;
-    rc = plain ? plain_gemm(m, nj, k, dA, pa, dB + (size_t)c0 * pb, pb, dC + (size_t)c0 * m, m, st)
-               : run_fmm(plan, pack, m, nj, k, dA, pa, dB + (size_t)c0 * pb, pb, dC + (size_t)c0 * m, m, st);
-    if (rc != FMM_OK) break;
-    if (P > 1) ok(cudaEventRecord(ev[1 + P + j], st)) && ok(cudaStreamWaitEvent(sout, ev[1 + P + j], 0));
+  cudaStream_t cin = NB > 1 ? sin : st, cout = NB > 1 ? sout : st;
+  if (rc == FMM_OK && NB > 1) ok(cudaEventRecord(ev[0], st)) && ok(cudaStreamWaitEvent(sin, ev[0], 0));
+  // block b = column panel b / R, row panel b % R
+  for (int b = 0; b < NB && rc == FMM_OK; ++b) {
+    const int i = b % R, j = b / R;
+    const int r0 = re[i], mi = re[i + 1] - re[i], c0 = ce[j], nj = ce[j + 1] - ce[j];
+    if (j == 0)  // A[I, :] at its first use
+      ok(cudaMemcpy2DAsync(dA + r0, sizeof(double) * pa, A + r0, sizeof(double) * lda, sizeof(double) * mi, k,
+                           cudaMemcpyHostToDevice, cin));
+    if (i == 0 && rc == FMM_OK)  // B[:, J] at its first use
+      ok(cudaMemcpy2DAsync(dB + (size_t)c0 * pb, sizeof(double) * pb, B + (size_t)c0 * ldb, sizeof(double) * ldb,
+                           sizeof(double) * k, nj, cudaMemcpyHostToDevice, cin));
     if (rc == FMM_OK)
-      ok(cudaMemcpy2DAsync(C + (size_t)c0 * ldc, sizeof(double) * ldc, dC + (size_t)c0 * m, sizeof(double) * m,
-                           sizeof(double) * m, nj, cudaMemcpyDeviceToHost, cout));
+      ok(cudaMemcpy2DAsync(dC + r0 + (size_t)c0 * m, sizeof(double) * m, C + r0 + (size_t)c0 * ldc,
+                           sizeof(double) * ldc, sizeof(double) * mi, nj, cudaMemcpyHostToDevice, cin));
+    if (NB > 1 && rc == FMM_OK) ok(cudaEventRecord(ev[1 + b], sin));
+  }
+  for (int b = 0; b < NB && rc == FMM_OK; ++b) {
+    const int i = b % R, j = b / R;
+    const int r0 = re[i], mi = re[i + 1] - re[i], c0 = ce[j], nj = ce[j + 1] - ce[j];
+    if (NB > 1 && !ok(cudaStreamWaitEvent(st, ev[1 + b], 0))) break;
+    double* Cb = dC + r0 + (size_t)c0 * m;
+    rc = plain ? plain_gemm(mi, nj, k, dA + r0, pa, dB + (size_t)c0 * pb, pb, Cb, m, st)
+               : run_fmm(plan, pack, mi, nj, k, dA + r0, pa, dB + (size_t)c0 * pb, pb, Cb, m, st);
+    if (rc != FMM_OK) break;
+    if (NB > 1) ok(cudaEventRecord(ev[1 + NB + b], st)) && ok(cudaStreamWaitEvent(sout, ev[1 + NB + b], 0));
+    if (rc == FMM_OK)
+      ok(cudaMemcpy2DAsync(C + r0 + (size_t)c0 * ldc, sizeof(double) * ldc, Cb, sizeof(double) * m,
+                           sizeof(double) * mi, nj, cudaMemcpyDeviceToHost, cout));
   }
   // join: every copy has finished before the buffers go back to the pool
   if (sin) ok(cudaStreamSynchronize(sin));

@@ -401,3 +401,24 @@ def test_gpu_presum_groups_match_oracle(oracle_lib, algs, levels, shape, limit):
     got = dC.cpu().numpy()
     assert rel_fro(got, want) <= RTOL_SMALL
     assert rel_fro(got, whole.cpu().numpy()) <= RTOL_SMALL
+
+
+def test_gpu_host_row_and_column_panels():
+    """A host call whose A is large enough for two row panels (C[I, J] += A[I, :] * B[:, J]
+    per block, half of A copied before the first kernel) matches the classical product within
+    rounding through the FMM and the plain kernel; the rows between m and ldc stay untouched."""
+    p = plan_for(["222"], [1])
+    m, n, k = 8200, 4610, 8192  # m * k >= 2^26: two row panels; n >= 2 * 2048: two column panels
+    rng = np.random.default_rng(8)
+    A = np.asfortranarray(rng.uniform(-1, 1, (m, k)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    Cbig = np.asfortranarray(rng.uniform(-1, 1, (m + 3, n)))
+    want = Cbig[:m] + A @ B
+    for pack in ("abc", None):
+        got = Cbig.copy(order="F")
+        if pack is None:
+            rt.bl_dgemm_host(A, B, got[:m])
+        else:
+            rt.fmm_gemm_host(p, A, B, got[:m], pack)
+        assert rel_fro(got[:m], want) <= RTOL_SMALL, pack
+        assert np.array_equal(got[m:], Cbig[m:]), pack
