@@ -266,8 +266,11 @@ void ksplit_build(const fmm_plan* p, int base, int S, std::vector<fmm::Prod>* op
   const std::vector<fmm::Prod>& prods = base == BASE_PS ? p->prods_ps : base == BASE_ALL ? p->prods_all : p->prods;
   const std::vector<fmm::Term>& terms = base == BASE_PS ? p->terms_ps : base == BASE_ALL ? p->terms_all : p->terms;
   std::vector<int> cnt((size_t)p->dims[0] * p->dims[2], 0);
-  for (const fmm::Prod& pr : prods) {
-    for (int q = 0; q < S; ++q) {
+  // part-major: split product (r, q) is q * R + r, so the S parts of one (tile, product) are
+  // R tiles' worth of units apart and do not run at the same time (their C updates are
+  // ordered by tickets, so parts claimed together would wait on each other)
+  for (int q = 0; q < S; ++q) {
+    for (const fmm::Prod& pr : prods) {
       fmm::Prod v = pr;
       v.a0 = (int)ot->size();
       for (int t = 0; t < pr.na; ++t) {
@@ -691,9 +694,12 @@ int choose_chunks(int ntiles, int nprod, int nsm) {
 // keep S = 1.
 constexpr int kUnitOverheadSteps = 4;  // per-unit cost beyond its k steps (hand-off, C tile traffic)
 constexpr int kMinPartSteps = 16;
+std::atomic<int> g_force_ksplit{0};  // fmm_debug_set FMM_DEBUG_KSPLIT: S for every split launch (0: model)
 int choose_ksplit(long long units, int ks, int nsm) {
   if (units <= 0 || nsm <= 0 || units >= 8LL * nsm || ks % fmm::BK != 0) return 1;
   const long long nks = ks / fmm::BK;
+  const int forced = g_force_ksplit.load();
+  if (forced > 0) return (nks % forced == 0 && nks / forced >= kMinPartSteps) ? forced : 1;
   auto cost = [&](int S) { return ((units * S + nsm - 1) / nsm) * (double)(nks / S + kUnitOverheadSteps); };
   int best = 1;
   double best_cost = cost(1);
@@ -1780,6 +1786,10 @@ int fmm_debug_set(int what, long long value) {
     case FMM_DEBUG_TICKET_FILL:
       if (value < 0 || value > 255) return FMM_E_INVALID;
       g_ticket_fill = (int)value;
+      return FMM_OK;
+    case FMM_DEBUG_KSPLIT:
+      if (value < 0 || value > 8) return FMM_E_INVALID;
+      g_force_ksplit = (int)value;
       return FMM_OK;
     case FMM_DEBUG_COMBINE_POSITIONS:
       if (value < 0 || value > 2) return FMM_E_INVALID;

@@ -139,11 +139,15 @@ long long fmm_last_workspace_bytes(void);
  *   FMM_DEBUG_COMBINE_POSITIONS: form of the stored-products combine pass: 0 (default) the
  *     shared-memory-staged form where the operands allow it, 1 or 2 the register form with
  *     that many element positions per thread; results are unchanged, for sweeps.
+ *   FMM_DEBUG_KSPLIT: k split S (1..8) of every launch the model would consider splitting
+ *     (launches of few waves); 0 restores the model's choice.  For sweeps; results change
+ *     within rounding.
  * Process-wide settings for tests; restore them before other work.  FMM_E_INVALID for an
- * unknown setting, a fill outside 0..255 or a position count outside 0..2. */
+ * unknown setting or a value outside its range. */
 #define FMM_DEBUG_WAIT_LIMIT_NS 1
 #define FMM_DEBUG_TICKET_FILL 2
 #define FMM_DEBUG_COMBINE_POSITIONS 3
+#define FMM_DEBUG_KSPLIT 4
 int fmm_debug_set(int what, long long value);
 
 /* FMM C += A*B (pack type ABC) that allocates no memory -- no counterpart in the
