@@ -1843,20 +1843,21 @@ __global__ void __launch_bounds__(CST_THREADS + 32) fmm_combine_staged_kernel(co
         const double* cf = sc + (size_t)ch * COMBINE_GROUP * CST_CHUNK;
         mbar_wait(full0 + 8 * s, (unsigned)((k / CST_STAGES) & 1), status);
         const double* st = stages + (size_t)s * CST_STAGE_DOUBLES + tid;
-        double m[CST_CHUNK];  // slots past the group's end hold stale data and have no bits
-#pragma unroll
-        for (int q = 0; q < CST_CHUNK; ++q) m[q] = st[(size_t)q * CST_TILE];
-        __threadfence_block();  // the stage's loads complete before it can be refilled
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty0 + 8 * s);  // the stage's values are in registers
+        // per member only its set slots (warp-uniform bit loops): the M value and the
+        // coefficient come from shared memory at the slot's index, the running value stays in
+        // a register (members unrolled); slots past the group's end have no bits
 #pragma unroll
         for (int b = 0; b < COMBINE_GROUP; ++b) {
-          const unsigned bq = (unsigned)(bits >> (8 * b)) & 0xffu;
-          if (bq == 0) continue;
-#pragma unroll
-          for (int q = 0; q < CST_CHUNK; ++q)
-            if (bq & (1u << q)) c[b] = fma(cf[b * CST_CHUNK + q], m[q], c[b]);
+          unsigned bq = (unsigned)(bits >> (8 * b)) & 0xffu;
+          while (bq) {
+            const int q = __ffs(bq) - 1;
+            bq &= bq - 1;
+            c[b] = fma(cf[b * CST_CHUNK + q], st[(size_t)q * CST_TILE], c[b]);
+          }
         }
+        __threadfence_block();  // the stage's loads complete before it can be refilled
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * s);
       }
       if (live) {
 #pragma unroll
