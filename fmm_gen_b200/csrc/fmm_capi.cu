@@ -694,6 +694,7 @@ int choose_chunks(int ntiles, int nprod, int nsm) {
 // keep S = 1.
 constexpr int kUnitOverheadSteps = 4;  // per-unit cost beyond its k steps (hand-off, C tile traffic)
 constexpr int kMinPartSteps = 16;
+std::atomic<int> g_split_form{0};     // fmm_debug_set FMM_DEBUG_SPLIT_OPERANDS: 1 = one product per CTA
 std::atomic<int> g_force_ksplit{0};  // fmm_debug_set FMM_DEBUG_KSPLIT: S for every split launch (0: model)
 int choose_ksplit(long long units, int ks, int nsm) {
   if (units <= 0 || nsm <= 0 || units >= 8LL * nsm || ks % fmm::BK != 0) return 1;
@@ -1032,8 +1033,21 @@ bool prefer_stored_products(const fmm_plan* plan, int ms, int ns, int ks) {
   return 1.08 * std::max(t_mma, t_store) + t_comb < 0.97 * t_direct;
 }
 
-int presum(const DevTables& d, const double* A, long long lda, const double* B, long long ldb, const PresumOps& ps,
-           int ms, int ns, int ks, cudaStream_t st) {
+// One operand's sums (fmm_lincomb_kernel): output j = blockIdx.x, element chunks over y.
+int launch_lincomb(const fmm_plan* plan, const fmm::LincombArgs& la, int nout, cudaStream_t st) {
+  (void)plan;
+  if (nout <= 0) return FMM_OK;
+  const long long pairs = (long long)(la.rows + 1) / 2 * la.cols;
+  {
+    ProfScope pf(K_LINCOMB, st);
+    fmm::fmm_lincomb_kernel<<<dim3((unsigned)nout, lincomb_chunks(pairs)), 256, 0, st>>>(la);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cuda_status(cudaGetLastError());
+}
+
+int presum(const fmm_plan* plan, const DevTables& d, const double* A, long long lda, const double* B, long long ldb,
+           const PresumOps& ps, int ms, int ns, int ks, cudaStream_t st) {
   if (ps.nslotA > 0) {
     fmm::LincombArgs la{};
     la.X = A;
@@ -1049,10 +1063,8 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     la.terms = d.terms;
     la.plist = ps.plistA ? ps.plistA : d.plistA;
     la.side = 0;
-    const dim3 g((unsigned)ps.nslotA, lincomb_chunks((long long)(ms + 1) / 2 * ks));
-    ProfScope pf(K_LINCOMB, st);
-    fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(la);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const int rc = launch_lincomb(plan, la, ps.nslotA, st);
+    if (rc != FMM_OK) return rc;
   }
   if (ps.nslotB > 0) {
     fmm::LincombArgs lb{};
@@ -1069,10 +1081,8 @@ int presum(const DevTables& d, const double* A, long long lda, const double* B, 
     lb.terms = d.terms;
     lb.plist = ps.plistB ? ps.plistB : d.plistB;
     lb.side = 1;
-    const dim3 g((unsigned)ps.nslotB, lincomb_chunks((long long)(ks + 1) / 2 * ns));
-    ProfScope pf(K_LINCOMB, st);
-    fmm::fmm_lincomb_kernel<<<g, 256, 0, st>>>(lb);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const int rc = launch_lincomb(plan, lb, ps.nslotB, st);
+    if (rc != FMM_OK) return rc;
   }
   return cuda_status(cudaGetLastError());
 }
@@ -1133,7 +1143,7 @@ int presum_prepare(const fmm_plan* plan, const DevTables& d, const double* A, lo
     out->terms = d.terms_ps;
     out->kk = ks;
   }
-  if (rc == FMM_OK) rc = presum(d, A, lda, B, ldb, ps, ms, ns, ks, st);
+  if (rc == FMM_OK) rc = presum(plan, d, A, lda, B, ldb, ps, ms, ns, ks, st);
   return rc;
 }
 
@@ -1217,7 +1227,7 @@ int run_presum_groups(const fmm_plan* plan, const DevTables& d, const double* A,
     ps.ldT = kk;
     ps.nslotB = n;
     if (g >= 2 && !ok(cudaStreamWaitEvent(side, ev_done[b], 0))) break;
-    rc = presum(d, A, lda, B, ldb, ps, ms, ns, ks, side);
+    rc = presum(plan, d, A, lda, B, ldb, ps, ms, ns, ks, side);
     if (!ok(cudaEventRecord(ev_sum[b], side)) || !ok(cudaStreamWaitEvent(st, ev_sum[b], 0))) break;
     const fmm::Prod* gp = nullptr;
     const fmm::Term* gt = nullptr;
@@ -1350,12 +1360,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         la.terms = d->terms;
         la.side = 0;
         la.plist = nullptr;
-        const dim3 ga((unsigned)R, lincomb_chunks((long long)(ms + 1) / 2 * ks));
-        {
-          ProfScope ps(K_LINCOMB, st);
-          fmm::fmm_lincomb_kernel<<<ga, 256, 0, st>>>(la);
-        }
-        g_launches.fetch_add(1, std::memory_order_relaxed);
+        rc = launch_lincomb(plan, la, R, st);
         fmm::LincombArgs lb = la;
         lb.X = B;
         lb.ldx = ldb;
@@ -1367,13 +1372,7 @@ int run_fmm(const fmm_plan* plan, int pack, int m, int n, int k, const double* A
         lb.ldo = ks;
         lb.out_stride = (long long)ks * ns;
         lb.side = 1;
-        const dim3 gb((unsigned)R, lincomb_chunks((long long)(ks + 1) / 2 * ns));
-        {
-          ProfScope ps(K_LINCOMB, st);
-          fmm::fmm_lincomb_kernel<<<gb, 256, 0, st>>>(lb);
-        }
-        g_launches.fetch_add(1, std::memory_order_relaxed);
-        rc = cuda_status(cudaGetLastError());
+        if (rc == FMM_OK) rc = launch_lincomb(plan, lb, R, st);
         // Product r: M_r = S_r * T_r, with S_r the block (0, r) of an ms x (R*ks) matrix.
         if (rc == FMM_OK) {
           DevTables* dc = nullptr;
@@ -1787,6 +1786,10 @@ int fmm_debug_set(int what, long long value) {
       if (value < 0 || value > 255) return FMM_E_INVALID;
       g_ticket_fill = (int)value;
       return FMM_OK;
+    case FMM_DEBUG_SPLIT_OPERANDS:
+      if (value < 0 || value > 1) return FMM_E_INVALID;
+      g_split_form = (int)value;
+      return FMM_OK;
     case FMM_DEBUG_KSPLIT:
       if (value < 0 || value > 8) return FMM_E_INVALID;
       g_force_ksplit = (int)value;
@@ -2064,6 +2067,10 @@ int split_configure(int* dev_out) {
   if (!split_configured[*dev_out]) {
     FMM_CUDA_TRY(cudaFuncSetAttribute(fmms::fmm_split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fmms::SMEM_BYTES));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmms::fmm_split_all_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      100 * 1024));
+    FMM_CUDA_TRY(cudaFuncSetAttribute(fmms::fmm_split_all_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      100 * 1024));
     split_configured[*dev_out] = true;
   }
   return g_encode_tiled ? FMM_OK : FMM_E_UNSUPPORTED;
@@ -2137,7 +2144,21 @@ int split_core(const fmm_plan* plan, const DevTables& d, const float* A, long lo
   sb.blk_col_stride = ns;
   sb.out = PB;
   sb.side = 1;
-  if (rc == FMM_OK) {
+  // every product's sums from one read of each operand, where the staged tiles fit
+  int nta = 0, ntb = 0;
+  for (const auto& pr : plan->prods) nta += pr.na, ntb += pr.nb;
+  const int nblk_a = plan->dims[0] * plan->dims[1], nblk_b = plan->dims[1] * plan->dims[2];
+  const size_t sm_a = fmms::split_all_smem_bytes(0, nblk_a, R, nta), sm_b = fmms::split_all_smem_bytes(1, nblk_b, R, ntb);
+  const bool all_form = g_split_form.load() == 0 && sm_a <= 100 * 1024 && sm_b <= 100 * 1024 && kpad % 64 == 0;
+  if (rc == FMM_OK && all_form) {
+    fmms::SplitAllArgs ga{sa, nblk_a, plan->dims[1], R, nta};
+    fmms::SplitAllArgs gb{sb, nblk_b, plan->dims[2], R, ntb};
+    ProfScope pf(K_SPLIT_OPERANDS, st);
+    fmms::fmm_split_all_kernel<0><<<dim3((unsigned)(kpad / 32), (unsigned)((ms + 15) / 16)), 256, sm_a, st>>>(ga);
+    fmms::fmm_split_all_kernel<1><<<dim3((unsigned)(kpad / 64), (unsigned)((ns + 7) / 8)), 256, sm_b, st>>>(gb);
+    g_launches.fetch_add(2, std::memory_order_relaxed);
+    rc = cuda_status(cudaGetLastError());
+  } else if (rc == FMM_OK) {
     ProfScope pf(K_SPLIT_OPERANDS, st);
     const dim3 blk(32, 8);
     const unsigned kt = (unsigned)(kpad / fmms::SPLIT_K);

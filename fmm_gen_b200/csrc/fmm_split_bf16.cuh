@@ -466,4 +466,113 @@ __global__ void __launch_bounds__(256) fmm_split_operands_kernel(const SplitArgs
   }
 }
 
+// Every product's operand sum from one read of the operand: a CTA stages one tile position of
+// all the operand's blocks (side 0: 16 rows x 32 k of each A block, side 1: 8 columns x 64 k
+// of each B block) in shared memory in the output orientation (row, k), then makes all R
+// products' sums of that tile in FP64 in term order (the same arithmetic as
+// fmm_split_operands_kernel, so the planes are bit-identical) and stores their three bf16
+// planes.  Each input element is read from HBM once and no CTA waits on a global load per
+// term: the per-product kernel read each block once per product that uses it.
+//   tables (shared memory): per product its first term and term count; per term its block
+//   (row * block_cols + col of the operand's block grid) and coefficient.
+template <int SIDE>
+struct SplitAllShape;
+template <>
+struct SplitAllShape<0> {  // A: 16 rows x 32 k, loads coalesced along rows
+  static constexpr int TR = 16, TK = 32;
+};
+template <>
+struct SplitAllShape<1> {  // B: 8 columns x 64 k, loads coalesced along k
+  static constexpr int TR = 8, TK = 64;
+};
+
+struct SplitAllArgs {
+  SplitArgs s;
+  int nblk, block_cols;  // the operand's block grid: nblk blocks, block_cols per block row
+  int nprod;
+  int nterm;             // sum of the products' term counts on this side
+};
+
+__host__ __device__ constexpr size_t split_all_smem_bytes(int side, int nblk, int nprod, int nterm) {
+  return sizeof(float) * (size_t)nblk * (side == 0 ? 16 * 33 : 8 * 65) + sizeof(int) * (2 * (size_t)nprod + nterm) +
+         sizeof(double) * (size_t)nterm + 16;
+}
+
+template <int SIDE>
+__global__ void __launch_bounds__(256) fmm_split_all_kernel(const SplitAllArgs g) {
+  constexpr int TR = SplitAllShape<SIDE>::TR, TK = SplitAllShape<SIDE>::TK, LD = TK + 1;
+  const SplitArgs& a = g.s;
+  extern __shared__ __align__(16) double sall[];
+  double* tcoef = sall;                                      // [nterm]
+  int* tblk = reinterpret_cast<int*>(tcoef + g.nterm);       // [nterm]
+  int* tfirst = tblk + g.nterm;                              // [nprod]
+  int* tcount = tfirst + g.nprod;                            // [nprod]
+  float* x = reinterpret_cast<float*>(tcount + g.nprod);     // [nblk][TR][LD]
+  const int tid = threadIdx.x;
+  // tables: term counts in parallel, offsets by one thread (shared memory only), terms in parallel
+  for (int r = tid; r < g.nprod; r += blockDim.x) {
+    const Prod p = a.prods[r];
+    tcount[r] = SIDE == 0 ? p.na : p.nb;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int r = 0; r < g.nprod; ++r) {
+      tfirst[r] = acc;
+      acc += tcount[r];
+    }
+  }
+  __syncthreads();
+  for (int r = tid; r < g.nprod; r += blockDim.x) {
+    const Prod p = a.prods[r];
+    const int t0 = SIDE == 0 ? p.a0 : p.b0, nt = tcount[r], f = tfirst[r];
+    for (int t = 0; t < nt; ++t) {
+      const Term tm = a.terms[t0 + t];
+      tcoef[f + t] = tm.coef;
+      tblk[f + t] = tm.row * g.block_cols + tm.col;
+    }
+  }
+  const int row0 = blockIdx.y * TR, k0 = blockIdx.x * TK;
+  // stage every block's tile, output orientation x[b][row][k]; zeros outside the block
+  for (int b = 0; b < g.nblk; ++b) {
+    const int br = b / g.block_cols, bc = b % g.block_cols;
+    float* xb = x + (size_t)b * TR * LD;
+    if (SIDE == 0) {  // A[(br ms + i) + (bc ks + k) lda]: lanes along i
+      const int i = tid % TR;
+#pragma unroll
+      for (int kk = tid / TR; kk < TK; kk += 256 / TR) {
+        const int row = row0 + i, k = k0 + kk;
+        xb[i * LD + kk] = (row < a.rows && k < a.ks)
+                              ? a.X[(long long)br * a.blk_row_stride + row + ((long long)bc * a.blk_col_stride + k) * a.ldx]
+                              : 0.0f;
+      }
+    } else {  // B[(br ks + k) + (bc ns + j) ldb]: lanes along k
+      const int kk = tid % TK;
+#pragma unroll
+      for (int j = tid / TK; j < TR; j += 256 / TK) {
+        const int row = row0 + j, k = k0 + kk;
+        xb[j * LD + kk] = (row < a.rows && k < a.ks)
+                              ? a.X[(long long)br * a.blk_row_stride + k + ((long long)bc * a.blk_col_stride + row) * a.ldx]
+                              : 0.0f;
+      }
+    }
+  }
+  __syncthreads();
+  // one k pair per thread: rows TR x TK / 2 pairs = 256
+  const int row = tid / (TK / 2), kk = 2 * (tid % (TK / 2));
+  if (row0 + row >= a.rows) return;
+  const float* xr = x + row * LD + kk;
+  for (int r = 0; r < g.nprod; ++r) {
+    double v0 = 0.0, v1 = 0.0;
+    const int f = tfirst[r], nt = tcount[r];
+    for (int t = 0; t < nt; ++t) {
+      const float* xp = xr + (size_t)tblk[f + t] * TR * LD;
+      const double w = tcoef[f + t];
+      v0 = fma(w, (double)xp[0], v0);
+      v1 = fma(w, (double)xp[1], v1);
+    }
+    store_split_pair(a, r, row0 + row, k0 + kk, v0, v1);
+  }
+}
+
 }  // namespace fmms

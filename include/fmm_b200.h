@@ -142,12 +142,16 @@ long long fmm_last_workspace_bytes(void);
  *   FMM_DEBUG_KSPLIT: k split S (1..8) of every launch the model would consider splitting
  *     (launches of few waves); 0 restores the model's choice.  For sweeps; results change
  *     within rounding.
+ *   FMM_DEBUG_SPLIT_OPERANDS: how the split-BF16 path forms its operand planes: 0 (default)
+ *     every product's sums from one staged read of each operand, 1 one product per CTA (the
+ *     two give identical planes; for tests and sweeps).
  * Process-wide settings for tests; restore them before other work.  FMM_E_INVALID for an
  * unknown setting or a value outside its range. */
 #define FMM_DEBUG_WAIT_LIMIT_NS 1
 #define FMM_DEBUG_TICKET_FILL 2
 #define FMM_DEBUG_COMBINE_POSITIONS 3
 #define FMM_DEBUG_KSPLIT 4
+#define FMM_DEBUG_SPLIT_OPERANDS 5
 int fmm_debug_set(int what, long long value);
 
 /* FMM C += A*B (pack type ABC) that allocates no memory -- no counterpart in the

@@ -165,3 +165,33 @@ def test_split_full_size_222_2_8192():
     torch.cuda.synchronize()
     assert rt.load_library().fmm_device_status(1) == 0
     assert ((C - ref).norm() / ref.norm()).item() <= RTOL_SPLIT
+
+
+@pytest.mark.parametrize("algs,levels,shape", [
+    (["222"], [2], (1000, 900, 1100)),        # 16 blocks per operand, fringes on every side
+    (["333"], [1], (700, 650, 610)),           # 9 blocks
+    (["222", "333"], [1, 1], (1210, 1190, 1300)),  # 36 blocks: the largest staged tile
+    (["222"], [1], (4100, 4097, 4103)),
+])
+def test_split_operand_forms_are_bit_identical(algs, levels, shape):
+    """The operand planes formed from one staged read of each operand (all products per tile,
+    the default) and one product per CTA give the same result bit for bit."""
+    m, n, k = shape
+    lib = rt.load_library()
+    p = rt.Plan.from_levels(algs, levels)
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    A = rt.colmajor(m, k, dtype=torch.float32, device="cuda").normal_(generator=g)
+    B = rt.colmajor(k, n, dtype=torch.float32, device="cuda").normal_(generator=g)
+    C0 = rt.colmajor(m, n, device="cuda").uniform_(-1, 1, generator=g)
+    out = []
+    try:
+        for form in (0, 1):
+            assert lib.fmm_debug_set(5, form) == 0
+            C = rt.colmajor(m, n, device="cuda").copy_(C0)
+            rt.split_gemm(p, A, B, C)
+            torch.cuda.synchronize()
+            out.append(C)
+    finally:
+        assert lib.fmm_debug_set(5, 0) == 0
+    assert lib.fmm_device_status(1) == 0
+    assert torch.equal(out[0], out[1])
