@@ -71,10 +71,11 @@ static inline double upd(double c, double w, double acc) {
   return c + w * acc;
 }
 
+#define MAX_TERMS 1024 /* operand / C terms of one product (three-level plans reach 1000) */
 typedef struct {
   int nt;
-  const double *src[64];
-  double coef[64];
+  const double *src[MAX_TERMS];
+  double coef[MAX_TERMS];
   long ld;
 } opnd_t;
 
@@ -242,7 +243,7 @@ int oracle_fmm(int pack, const int *dims, int R, const int *nterms, const int *r
     int pos = 0;
     for (int r = 0; r < R && rc == 0; ++r) {
       const int na = nterms[3 * r], nb = nterms[3 * r + 1], nc = nterms[3 * r + 2];
-      if (na > 64 || nb > 64 || nc > 64) {
+      if (na > MAX_TERMS || nb > MAX_TERMS || nc > MAX_TERMS) {
         rc = -6;
         break;
       }
@@ -259,8 +260,8 @@ int oracle_fmm(int pack, const int *dims, int R, const int *nterms, const int *r
         b.src[t] = B + (long)rows[pos] * ks + (long)cols[pos] * ns * ldb;
         b.coef[t] = coefs[pos];
       }
-      double *cd[64];
-      double w[64];
+      double *cd[MAX_TERMS];
+      double w[MAX_TERMS];
       for (int t = 0; t < nc; ++t, ++pos) {
         cd[t] = C + (long)rows[pos] * ms + (long)cols[pos] * ns * ldc;
         w[t] = coefs[pos];

@@ -97,6 +97,8 @@ ORACLE_CASES = [
     (["222"], [1], (2056, 2052, 606)),
     (["333"], [1], (3080, 3090, 800)),
     (["424"], [1], (4104, 2060, 1034)),
+    # 336 at two levels: 100 operand terms per product side (beyond the sums' staged term table)
+    (["336"], [2], (3000, 14420, 910)),
 ]
 
 
