@@ -972,7 +972,7 @@ int launch_combine(const fmm_plan* plan, const DevTables& d, double* C, long lon
                       ((uintptr_t)M & 15) == 0 && ssm <= 200 * 1024 && total > 0;
   if (staged) {
     const long long ntile = (total + fmm::CST_TILE - 1) / fmm::CST_TILE;
-    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(ntile, (long long)sm_count[dev] * 2));
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(ntile, (long long)sm_count[dev] * 3));
     {
       ProfScope pf(K_COMBINE, st);
       fmm::fmm_combine_staged_kernel<<<grid, fmm::CST_THREADS + 32, ssm, st>>>(ga, dev_status[dev]);

@@ -1743,7 +1743,7 @@ __global__ void __launch_bounds__(COMBINE_G_THREADS) fmm_combine_kernel(const Co
 constexpr int CST_THREADS = 256;  // compute threads, one position each
 constexpr int CST_TILE = CST_THREADS;
 constexpr int CST_CHUNK = 8;      // products per stage
-constexpr int CST_STAGES = 5;
+constexpr int CST_STAGES = 3;  // 48 KB of stages: three CTAs per SM (24 compute warps)
 constexpr size_t CST_STAGE_DOUBLES = (size_t)CST_CHUNK * CST_TILE;
 static_assert(COMBINE_GROUP * CST_CHUNK <= 64, "one 64-bit word of slot bits per chunk");
 
