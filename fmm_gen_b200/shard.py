@@ -134,3 +134,53 @@ class Gemm2D:
         B = self.gather_b(B_own)
         if C_own.numel():
             local_gemm(A, B, C_own)
+
+    def k_chunks(self) -> List[Tuple[int, int]]:
+        """The k range cut at every edge of both starting distributions: each chunk lies in one
+        rank's A slice (of this grid row) and in one rank's B slice (of this grid column)."""
+        edges = sorted({e for ab in (self.blk.a_ks, self.blk.b_ks) for r in ab for e in r})
+        return [(e0, e1) for e0, e1 in zip(edges, edges[1:]) if e1 > e0]
+
+    def run_pipelined(self, A_own, B_own, C_own, local_gemm: Callable) -> None:
+        """C[I_i, J_j] += A[I_i, :] * B[:, J_j] in k chunks (a SUMMA order): the owner of a chunk's
+        A[I_i, K_q] broadcasts it over the grid row and the owner of B[K_q, J_j] over the grid
+        column, and chunk q + 1's broadcasts are in flight while chunk q's local GEMM runs.  The
+        exchange then hides behind the compute; each chunk is a GEMM of its own, so the rounding
+        differs from run()'s (within the same error bound)."""
+        import torch
+
+        dist, blk = self.dist, self.blk
+        rows = blk.rows[1] - blk.rows[0]
+        cols = blk.cols[1] - blk.cols[0]
+        chunks = self.k_chunks()
+        owner_a = [next(j for j, (a, b) in enumerate(blk.a_ks) if a <= k0 and k1 <= b) for k0, k1 in chunks]
+        owner_b = [next(i for i, (a, b) in enumerate(blk.b_ks) if a <= k0 and k1 <= b) for k0, k1 in chunks]
+
+        def fetch(q):
+            k0, k1 = chunks[q]
+            w = k1 - k0
+            works = []
+            # A[I, K_q] column-major = a row-major (w, rows) buffer
+            if owner_a[q] == blk.j:
+                a = A_own[:, k0 - blk.a_k[0]:k1 - blk.a_k[0]].t().contiguous()
+            else:
+                a = torch.empty((w, rows), dtype=A_own.dtype, device=A_own.device)
+            if self.pc > 1:
+                works.append(dist.broadcast(a, src=blk.i * self.pc + owner_a[q], group=self.row_group, async_op=True))
+            # B[K_q, J] column-major = a row-major (cols, w) buffer
+            if owner_b[q] == blk.i:
+                b = B_own[k0 - blk.b_k[0]:k1 - blk.b_k[0], :].t().contiguous()
+            else:
+                b = torch.empty((cols, w), dtype=B_own.dtype, device=B_own.device)
+            if self.pr > 1:
+                works.append(dist.broadcast(b, src=owner_b[q] * self.pc + blk.j, group=self.col_group, async_op=True))
+            return a, b, works
+
+        nxt = fetch(0) if chunks else None
+        for q in range(len(chunks)):
+            a, b, works = nxt
+            for wk in works:
+                wk.wait()
+            nxt = fetch(q + 1) if q + 1 < len(chunks) else None
+            if C_own.numel():
+                local_gemm(a.t(), b.t(), C_own)

@@ -1,7 +1,7 @@
 """One GEMM split 2-D over ranks (fmm_gen_b200.shard), as gloo process groups on the CPU:
 each rank starts with one k slice of its A row panel and of its B column panel, gathers both
-panels over its grid row / column, and computes its C block; the assembled C equals
-C0 + A*B.  The local GEMM here is torch's FP64 CPU matmul (on GPUs it is the library's FMM)."""
+panels over its grid row / column (or, in k chunks, receives each chunk from its owner while the
+previous chunk computes), and computes its C block; the assembled C equals C0 + A*B.  The local GEMM here is torch's FP64 CPU matmul (on GPUs it is the library's FMM)."""
 import os
 import socket
 
@@ -25,7 +25,7 @@ def _cm(x):
     return x.t().contiguous().t()
 
 
-def _worker(rank, world, port, shape, out):
+def _worker(rank, world, port, shape, out, pipelined=False):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -46,7 +46,7 @@ def _worker(rank, world, port, shape, out):
             assert Ap.stride(0) == 1 and Bp.stride(0) == 1
             Cp += Ap @ Bp
 
-        gm.run(A_own, B_own, C_own, local)
+        (gm.run_pipelined if pipelined else gm.run)(A_own, B_own, C_own, local)
         blocks = [None] * world
         dist.all_gather_object(blocks, (b.rows, b.cols, C_own.clone()))
         if rank == 0:
@@ -61,12 +61,13 @@ def _worker(rank, world, port, shape, out):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("pipelined", [False, True], ids=["gathered", "k_chunks"])
 @pytest.mark.parametrize("world,shape", [(2, (300, 520, 260)), (4, (384, 700, 333))])
-def test_2d_split_assembles_the_whole_product(world, shape):
+def test_2d_split_assembles_the_whole_product(world, shape, pipelined):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, shape, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, shape, q, pipelined)) for r in range(world)]
     for p in procs:
         p.start()
     covered, err, pr, pc = q.get(timeout=240)
