@@ -160,20 +160,27 @@ class Gemm2D:
             k0, k1 = chunks[q]
             w = k1 - k0
             works = []
-            # A[I, K_q] column-major = a row-major (w, rows) buffer
-            if owner_a[q] == blk.j:
-                a = A_own[:, k0 - blk.a_k[0]:k1 - blk.a_k[0]].t().contiguous()
+            # A[I, K_q]: a column-major view of this rank's slice when the grid row is this rank
+            # alone, else a row-major (w, rows) buffer (= column-major rows x w) broadcast by its owner
+            if self.pc == 1:
+                a = A_own[:, k0 - blk.a_k[0]:k1 - blk.a_k[0]]
             else:
-                a = torch.empty((w, rows), dtype=A_own.dtype, device=A_own.device)
-            if self.pc > 1:
-                works.append(dist.broadcast(a, src=blk.i * self.pc + owner_a[q], group=self.row_group, async_op=True))
-            # B[K_q, J] column-major = a row-major (cols, w) buffer
-            if owner_b[q] == blk.i:
-                b = B_own[k0 - blk.b_k[0]:k1 - blk.b_k[0], :].t().contiguous()
+                if owner_a[q] == blk.j:
+                    buf = A_own[:, k0 - blk.a_k[0]:k1 - blk.a_k[0]].t().contiguous()
+                else:
+                    buf = torch.empty((w, rows), dtype=A_own.dtype, device=A_own.device)
+                works.append(dist.broadcast(buf, src=blk.i * self.pc + owner_a[q], group=self.row_group, async_op=True))
+                a = buf.t()
+            # B[K_q, J] likewise (row-major (cols, w) buffer = column-major w x cols)
+            if self.pr == 1:
+                b = B_own[k0 - blk.b_k[0]:k1 - blk.b_k[0], :]
             else:
-                b = torch.empty((cols, w), dtype=B_own.dtype, device=B_own.device)
-            if self.pr > 1:
-                works.append(dist.broadcast(b, src=owner_b[q] * self.pc + blk.j, group=self.col_group, async_op=True))
+                if owner_b[q] == blk.i:
+                    buf = B_own[k0 - blk.b_k[0]:k1 - blk.b_k[0], :].t().contiguous()
+                else:
+                    buf = torch.empty((cols, w), dtype=B_own.dtype, device=B_own.device)
+                works.append(dist.broadcast(buf, src=owner_b[q] * self.pc + blk.j, group=self.col_group, async_op=True))
+                b = buf.t()
             return a, b, works
 
         nxt = fetch(0) if chunks else None
@@ -183,4 +190,4 @@ class Gemm2D:
                 wk.wait()
             nxt = fetch(q + 1) if q + 1 < len(chunks) else None
             if C_own.numel():
-                local_gemm(a.t(), b.t(), C_own)
+                local_gemm(a, b, C_own)
