@@ -21,8 +21,11 @@
 //        once and every element receives its products in order r = 0..R-1.
 //   * M_Add / S_Add / T_Add (meta/ab_gen_mix.py:341-372, meta/naive_gen_mix.py:60-137)
 //     -> fmm_lincomb_kernel / fmm_lincomb_batch_kernel (operand sums formed in HBM, also
-//        used by the ABC pack type for large sub-blocks), fmm_combine_kernel (every
-//        C_l += W[l,r] M_r of a batch of products in one pass), fmm_scatter_kernel.
+//        used by the ABC pack type for large sub-blocks), fmm_combine_staged_kernel and
+//        fmm_combine_kernel (every C_l += W[l,r] M_r of the stored products in one pass, the
+//        C blocks in groups that share products, running values in registers; the staged
+//        form brings the M tiles in by bulk copies), fmm_scatter_kernel (one C block per
+//        launch row, beyond the combine's tables).
 //   * The direct variant (fmm_gemm_direct_kernel) runs when every operand is a single
 //     aligned term (pre-summed operands): a deeper TMA pipeline and an epilogue on the
 //     producer warps that overlaps the next product's DMMA.
